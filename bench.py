@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Benchmark: time per 30-qubit depth-40 random circuit on one B200.
+
+Workload: the U(theta,phi,lambda)-per-qubit + CX brick-wall circuit, 30
+qubits, 40 layers (1200 U + 580 CX), seed 1234, complex64 state (8 GiB,
+larger than L2, so no flush is needed between steps), greedy fusion into
+k<=5-qubit blocks applied on the tensor cores (tcgen05, 3xTF32).  A step =
+ket::run semantics: reset to |0...0> and apply the whole circuit.
+
+Lines printed by rank 0 (one JSON line):
+  value        ms per circuit (device time, CUDA events on the state's
+               stream, K steps between barriers, max over ranks, / N for
+               the aggregate over N replicas)
+  e2e          the same through the C ABI with host buffers (ketgpu_run:
+               ops from host, the 2^30 amplitudes back into a host
+               complex128 buffer)
+  roofline     the dense-block kernel: algorithmic bytes per launch / its
+               mean CUDA-event duration, against MEASURED_PEAKS.json HBM
+  cpu_baseline ket itself (oracle/_ref/libket_ref.so, all host threads) on
+               a bounded sample of the same circuit, extrapolated
+  --impl reference   times ket's CPU path the same way and prints its line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as ct
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_QUBITS, DEPTH, SEED = 30, 40, 1234
+METRIC = "time per 30q circuit"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) >= 9:
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_baseline_reference(circ_ops, seconds_budget=20.0):
+    """ket::run (all host threads) on a bounded sample of the circuit.
+
+    The sample: ket::run of the empty 30-qubit circuit (state allocation),
+    then of prefixes holding only U gates and only CX gates; per-gate times
+    are extrapolated to the 1200 U + 580 CX of the full circuit.
+    """
+    from oracle.oracle import CODE, Reference
+    R = Reference()
+    R.set_num_threads(0)
+    cores = R.num_threads()
+    u_ops = circ_ops[circ_ops["type"] == CODE["U"]]
+    cx_ops = circ_ops[circ_ops["type"] == CODE["CX"]]
+    t0 = R.run_timed(N_QUBITS, circ_ops[:0])
+    t_u1 = R.run_timed(N_QUBITS, u_ops[:1])
+    per_u = max(t_u1 - t0, 1e-6)
+    k_u = int(max(1, min(8, (seconds_budget * 0.5) // per_u)))
+    tu = R.run_timed(N_QUBITS, u_ops[:k_u])
+    per_u = max((tu - t0) / k_u, 1e-6)
+    k_cx = int(max(1, min(8, (seconds_budget * 0.3) // per_u)))
+    tcx = R.run_timed(N_QUBITS, cx_ops[:k_cx])
+    per_cx = max((tcx - t0) / k_cx, 1e-6)
+    n_u, n_cx = len(u_ops), len(cx_ops)
+    est = t0 + per_u * n_u + per_cx * n_cx
+    return {
+        "value": est * 1e3, "unit": "ms/circuit", "cores": cores, "kind": "reference",
+        "sample": (f"ket::run (oracle/_ref/libket_ref.so, set_num_threads(0)) at 30 qubits complex128: "
+                   f"empty circuit {t0:.2f} s, {k_u} U gates {tu:.2f} s, {k_cx} CX gates {tcx:.2f} s; "
+                   f"extrapolated {t0:.2f} + {n_u} x {per_u:.3f} + {n_cx} x {per_cx:.3f} s"),
+    }
+
+
+def init_dist(n_gpus):
+    rank, world, local = 0, 1, 0
+    if n_gpus > 1 or "RANK" in os.environ:
+        import torch.distributed as dist
+        rank = int(os.environ.get("RANK", 0))
+        world = int(os.environ.get("WORLD_SIZE", 1))
+        local = int(os.environ.get("LOCAL_RANK", 0))
+        import datetime
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference_arm(args):
+    rank, world, _ = init_dist(args.gpus)
+    if rank != 0:
+        barrier(world)
+        return
+    from ket_b200.workloads import random_brickwork
+    ops = random_brickwork(N_QUBITS, DEPTH, SEED).to_ops()
+    vals = []
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    for _ in range(max(1, args.steps)):
+        vals.append(cpu_baseline_reference(ops, seconds_budget=10.0))
+    v = statistics.median([x["value"] for x in vals])
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "ms/circuit", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "random U+CX brick wall, 30 qubits, depth 40, seed 1234",
+                   "global_batch": 1, "seq_len": None, "parallelism": "replicas"},
+        "cpu_baseline": {"value": v, "unit": "ms/circuit", "cores": vals[0]["cores"], "kind": "reference",
+                         "sample": vals[0]["sample"]},
+        "e2e": {"value": v, "unit": "ms/circuit", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    barrier(world)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fusion", default="greedy")
+    ap.add_argument("--k", type=int, default=5)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    rank, world, local = init_dist(args.gpus)
+    import ket_b200 as ket
+    from ket_b200 import _lib
+    from ket_b200.workloads import random_brickwork
+    lib = _lib.lib
+
+    circ = random_brickwork(N_QUBITS, DEPTH, SEED)
+    ops = circ.to_ops()
+    opt = ket.make_options("c64", args.fusion, args.k, True)
+    plan = ket.Plan(N_QUBITS, ops, opt)
+    stats = plan.stats()
+    npass = int(stats["n_passes"])
+    info = []
+    for i in range(npass):
+        kind, k, tc, b = ct.c_int32(), ct.c_int32(), ct.c_int32(), ct.c_double()
+        _lib.check(lib.ketgpu_plan_pass_info(plan._h, i, ct.byref(kind), ct.byref(k), ct.byref(tc), ct.byref(b)))
+        info.append((kind.value, k.value, tc.value, b.value))
+    state = ket.DeviceState(N_QUBITS, "c64")
+    import torch
+    stream = torch.cuda.ExternalStream(lib.ketgpu_state_stream(state.handle))
+    pass_ms = np.zeros(npass, dtype=np.float32)
+
+    def step(timed_passes=None):
+        _lib.check(lib.ketgpu_state_reset(state.handle))
+        if timed_passes is not None:
+            _lib.check(lib.ketgpu_plan_execute_timed(plan._h, state.handle, timed_passes.ctypes.data))
+        else:
+            _lib.check(lib.ketgpu_plan_execute(plan._h, state.handle))
+
+    for _ in range(args.warmup):
+        step()
+    _lib.check(lib.ketgpu_state_synchronize(state.handle))
+    # per-pass timing (its own sweep, so the headline region has no extra events)
+    per_pass = []
+    for _ in range(2):
+        step(pass_ms)
+        per_pass.append(pass_ms.copy())
+    per_pass = np.mean(per_pass, axis=0)
+
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = Clocks(local) if rank == 0 else None
+    launches0 = ket.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    _lib.check(lib.ketgpu_state_synchronize(state.handle))
+    torch.cuda.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    launches = ket.launch_count() - launches0
+    clocks = clk.stop() if clk else None
+    ms_total = barrier_max(ms_total, world)
+    ms_step = ms_total / args.steps
+    value = ms_step / world  # aggregate: N circuits per step over N replicas
+
+    # correctness guard on the timed state: unit norm
+    nrm = state.norm()
+
+    # dense-block kernel roofline (tensor-core passes)
+    tc_idx = [i for i, x in enumerate(info) if x[0] == 2 and x[2] == 1]
+    peak, peak_kind = peaks()
+    roof = None
+    if tc_idx:
+        dur = float(np.mean(per_pass[tc_idx]))
+        byts = float(np.mean([info[i][3] for i in tc_idx]))
+        ach = byts / (dur * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "peak_source": peak_kind, "traffic": None, "kernel": "fused_tc_kernel<5>",
+                "bytes_per_launch": byts, "mean_launch_ms": dur, "launches_per_step": len(tc_idx)}
+    other = [i for i in range(npass) if i not in tc_idx]
+    pass_summary = {
+        "dense_tc_ms": float(per_pass[tc_idx].sum()) if tc_idx else 0.0,
+        "per_gate_ms": float(per_pass[other].sum()) if other else 0.0,
+        "hbm_gbs_all_passes": float(stats["bytes"] / (per_pass.sum() * 1e-3) / 1e9),
+    }
+
+    # e2e through the C ABI with host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        out = np.empty(1 << N_QUBITS, dtype=np.complex128)
+        ops_pinned = ops.copy()
+        ts = []
+        for i in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _lib.check(lib.ketgpu_run(N_QUBITS, ops_pinned.ctypes.data, len(ops_pinned), ct.byref(opt),
+                                      out.ctypes.data))
+            t1 = time.perf_counter()
+            if i > 0:
+                ts.append((t1 - t0) * 1e3)
+        e2e_ms = barrier_max(statistics.median(ts), world) / world
+        mat_bytes = int(stats["n_tensor"]) * 2 * 64 * 64 * 4
+        e2e = {"value": e2e_ms, "unit": "ms/circuit", "h2d_bytes_per_step": int(ops.nbytes) + mat_bytes,
+               "d2h_bytes_per_step": (1 << N_QUBITS) * 8,
+               "note": "ketgpu_run: host ops in, 2^30 amplitudes out to a host complex128 buffer"}
+        del out
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_reference(ops)
+        except Exception as ex:  # the reference build may be absent
+            cpu = {"value": None, "unit": "ms/circuit", "cores": None, "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "ms/circuit", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "random U+CX brick wall, 30 qubits, depth 40, seed 1234, complex64, "
+                                   f"{args.fusion} fusion k<={args.k} on tcgen05 3xTF32",
+                       "global_batch": world, "seq_len": None, "parallelism": f"replicas x{world}",
+                       "l2": "state 8 GiB > L2 126 MB, no flush", "gates": int(stats["n_gates"]),
+                       "passes": npass, "tensor_passes": int(stats["n_tensor"])},
+            "roofline": roof, "passes": pass_summary, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clocks, "norm": nrm,
+        }
+        print(json.dumps(line), flush=True)
+    state.close()
+    plan.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,223 @@
+/*
+ * ket_b200.h -- C ABI of the B200 state-vector backend for ket.
+ *
+ * The library (ket_b200/libket_b200.so) holds every CUDA kernel of the
+ * backend.  Its entry points take plain pointers and sizes only, so ket's
+ * C++ layer (or any FFI) can bind them without CUDA or torch headers.  Each
+ * declaration names the reference interface it replaces, as
+ * file:line within the ket sources.
+ *
+ * Conventions
+ *   - Every function returns KETGPU_OK (0) or a negative KETGPU_ERR_* code;
+ *     ketgpu_last_error() gives the calling thread's last message.  The
+ *     codes map onto the exceptions ket throws: OUT_OF_RANGE ->
+ *     std::out_of_range, INVALID -> std::invalid_argument, LOGIC ->
+ *     std::logic_error, anything else -> std::runtime_error.
+ *   - Host buffers of amplitudes are complex128 interleaved (re, im), index
+ *     bit q = qubit q (little-endian), exactly ket::State's layout
+ *     (include/ket/state.hpp:12-34).
+ *   - A ketgpu_state lives on the CUDA device that was current when it was
+ *     created; calls switch to that device and back.
+ *   - Calls that return a result to the host synchronise the state's stream;
+ *     ketgpu_plan_execute only enqueues.
+ */
+#ifndef KET_B200_H
+#define KET_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KETGPU_ABI_VERSION 1
+
+#define KETGPU_OK 0
+#define KETGPU_ERR_OUT_OF_RANGE (-1)
+#define KETGPU_ERR_INVALID (-2)
+#define KETGPU_ERR_LOGIC (-3)
+#define KETGPU_ERR_CUDA (-4)
+#define KETGPU_ERR_OOM (-5)
+#define KETGPU_ERR_TIMEOUT (-6)
+
+/* Gate codes: the numbering of ket::GateType (include/ket/gate.hpp:16-29). */
+enum ketgpu_gate {
+  KETGPU_H = 0, KETGPU_X, KETGPU_Y, KETGPU_Z, KETGPU_S, KETGPU_SDG, KETGPU_T,
+  KETGPU_TDG, KETGPU_RX, KETGPU_RY, KETGPU_RZ, KETGPU_U, KETGPU_CH, KETGPU_CX,
+  KETGPU_CY, KETGPU_CZ, KETGPU_CRX, KETGPU_CRY, KETGPU_CRZ, KETGPU_CU,
+  KETGPU_CP, KETGPU_SWAP, KETGPU_CCX, KETGPU_CSWAP, KETGPU_MEASURE,
+  KETGPU_BARRIER, KETGPU_COMPOSITE, KETGPU_PROBE
+};
+
+/* One circuit operation, the flattened form of ket::Gate
+ * (include/ket/gate.hpp:31-41): qubits in g.qubits order, params in
+ * g.params order.  Composite blocks are flattened by the caller (wire
+ * remap as in simulator.cpp:504-511).  For MEASURE, q[1] is the classical
+ * bit.  48 bytes. */
+typedef struct ketgpu_op {
+  int32_t type;
+  int32_t nq;
+  int32_t q[3];
+  int32_t aux;
+  double p[3];
+} ketgpu_op;
+
+enum ketgpu_precision { KETGPU_C64 = 0, KETGPU_C128 = 1 };
+
+enum ketgpu_fusion {
+  KETGPU_FUSE_NONE = 0,      /* one kernel per gate (the plain method) */
+  KETGPU_FUSE_REFERENCE = 1, /* ket's own block rule (simulator.cpp:400-477) */
+  KETGPU_FUSE_GREEDY = 2,    /* DAG-aware k-qubit blocks, static cost model */
+  KETGPU_FUSE_LEARNED = 3    /* k-qubit blocks scored by the MLP cost model */
+};
+
+typedef struct ketgpu_options {
+  int32_t precision;        /* ketgpu_precision */
+  int32_t fusion;           /* ketgpu_fusion */
+  int32_t max_block_qubits; /* k <= 6 (fused blocks); 0 = default (5) */
+  int32_t tensor_cores;     /* 1: complex64 blocks on tcgen05 (3xTF32); 0: SIMT */
+} ketgpu_options;
+
+typedef struct ketgpu_plan_stats {
+  uint64_t n_gates;         /* unitary gates in the circuit */
+  uint64_t n_passes;        /* kernels one execution launches */
+  uint64_t n_fused;         /* dense k-qubit block passes among them */
+  uint64_t n_tensor;        /* of those, on the tensor cores */
+  double bytes;             /* algorithmic HBM bytes of one execution */
+  double flops;             /* algorithmic flops of the fused blocks */
+  double predicted_us;      /* cost-model estimate (learned / greedy) */
+} ketgpu_plan_stats;
+
+typedef struct ketgpu_state ketgpu_state;
+typedef struct ketgpu_plan ketgpu_plan;
+typedef struct ketgpu_mlp ketgpu_mlp;
+
+/* ---- library --------------------------------------------------------- */
+const char* ketgpu_last_error(void);
+int ketgpu_abi_version(void);
+/* Number of launches of this library's kernels since load (all devices). */
+uint64_t ketgpu_launch_count(void);
+
+/* ---- state: replaces ket::State storage and ground_state
+ *      (include/ket/state.hpp:15-34, src/simulator.cpp:529-533) ---------- */
+int ketgpu_state_create(int32_t n_qubits, int32_t precision, ketgpu_state** out);
+int ketgpu_state_destroy(ketgpu_state* s);
+int ketgpu_state_reset(ketgpu_state* s); /* |0...0> */
+int ketgpu_state_info(const ketgpu_state* s, int32_t* n_qubits, int32_t* precision);
+/* Device pointer of the amplitudes (float2 or double2 per amplitude). */
+void* ketgpu_state_device_ptr(const ketgpu_state* s);
+/* Copy amplitudes [first, first+count) to a host complex128 buffer. */
+int ketgpu_state_download(const ketgpu_state* s, uint64_t first, uint64_t count,
+                          double* out_c128);
+/* Overwrite amplitudes [first, first+count) from a host complex128 buffer. */
+int ketgpu_state_upload(ketgpu_state* s, uint64_t first, uint64_t count,
+                        const double* in_c128);
+int ketgpu_state_copy(const ketgpu_state* src, ketgpu_state* dst);
+int ketgpu_state_synchronize(ketgpu_state* s);
+
+/* ---- circuits: replaces ket::run / apply_circuit / Fuser
+ *      (include/ket/simulator.hpp:15, src/simulator.cpp:400-558) --------- */
+int ketgpu_plan_create(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
+                       const ketgpu_options* opt, ketgpu_plan** out);
+int ketgpu_plan_destroy(ketgpu_plan* p);
+int ketgpu_plan_stats_get(const ketgpu_plan* p, ketgpu_plan_stats* out);
+/* Enqueue every pass of the plan on the state's stream (no host sync). */
+int ketgpu_plan_execute(const ketgpu_plan* p, ketgpu_state* s);
+/* Execute and time every pass with CUDA events on the state's stream;
+ * pass_ms receives n_passes durations (milliseconds).  Synchronises. */
+int ketgpu_plan_execute_timed(const ketgpu_plan* p, ketgpu_state* s, float* pass_ms);
+/* Describe pass `index`: kind (0 pair, 1 phase, 2 dense block), block
+ * qubits k, tensor-core flag and algorithmic HBM bytes. */
+int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* kind, int32_t* k,
+                          int32_t* tensor, double* bytes);
+/* The state's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or events against the backend's. */
+void* ketgpu_state_stream(const ketgpu_state* s);
+/* Plan + execute + synchronise. */
+int ketgpu_apply(ketgpu_state* s, const ketgpu_op* ops, uint64_t n_ops,
+                 const ketgpu_options* opt);
+/* ket::run with host buffers: |0...0>, the circuit, then the 2^n amplitudes
+ * as complex128 into out_c128 (simulator.hpp:15, simulator.cpp:554-558). */
+int ketgpu_run(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
+               const ketgpu_options* opt, double* out_c128);
+
+/* ---- reductions (FP64 accumulation) --------------------------------- */
+int ketgpu_norm(const ketgpu_state* s, double* out);
+/* <a|b> (complex) -- fidelity checks. */
+int ketgpu_inner(const ketgpu_state* a, const ketgpu_state* b, double* re, double* im);
+/* Replaces ket::expval(State, string) (include/ket/observable.hpp:24,
+ * src/observable.cpp:18-83): same masks, same right-to-left order, same
+ * errors (length / character -> KETGPU_ERR_INVALID). */
+int ketgpu_expval(const ketgpu_state* s, const char* pauli, double* out);
+/* Replaces ket::expval(State, PauliSum) (include/ket/observable.hpp:32,
+ * src/observable.cpp:85-91); every term in one batched reduction. */
+int ketgpu_expval_sum(const ketgpu_state* s, const double* coeffs,
+                      const char* const* paulis, uint64_t n_terms, double* out);
+/* Per-term expectations (out has n_terms entries). */
+int ketgpu_expval_terms(const ketgpu_state* s, const char* const* paulis,
+                        uint64_t n_terms, double* out);
+
+/* ---- sampling: replaces ket::measure (include/ket/measurement.hpp:16-17,
+ *      src/measurement.cpp:12-21) ------------------------------------- */
+/* The draws ket::measure consumes: uniform_real_distribution<double>(0,1)
+ * on std::mt19937{seed}, `count` of them in order. */
+int ketgpu_uniforms_mt19937(uint32_t seed, uint64_t count, double* out);
+/* Born-rule draws for the given uniforms (host arrays), one FP64 CDF built
+ * once over a fixed summation tree (segments of 32, carries folded
+ * top-down), each draw the first index whose running sum exceeds u. */
+int ketgpu_sample(const ketgpu_state* s, const double* uniforms, uint64_t count,
+                  uint64_t* out_indices);
+/* One draw from std::mt19937{seed} (measurement.cpp:12-21 with a seeded rng). */
+int ketgpu_measure(const ketgpu_state* s, uint32_t seed, uint64_t* out_index);
+
+/* ---- adjoint differentiation (no ket counterpart; gradients of
+ *      ket::expval(run(circuit(theta)), PauliSum)) ----------------------
+ * param_index[i] >= 0 marks op i's first angle as parameter param_index[i]
+ * (Rx, Ry, Rz, CRx, CRy, CRz, CP).  params: batch x n_params (row-major);
+ * values: batch; grads: batch x n_params.  checkpoint_every > 0 stores the
+ * forward state every that many parameterised layers and restarts the
+ * reverse sweep's state from the checkpoints. */
+int ketgpu_adjoint(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
+                   const int32_t* param_index, const double* params,
+                   uint64_t n_params, uint64_t batch, const double* coeffs,
+                   const char* const* paulis, uint64_t n_terms,
+                   int32_t precision, int32_t checkpoint_every, double* values,
+                   double* grads);
+
+/* ---- learned fusion cost model (48 -> 128 -> 128 -> 1 MLP, BF16 weights,
+ *      FP32 accumulation; no ket counterpart) ------------------------- */
+#define KETGPU_MLP_IN 48
+#define KETGPU_MLP_HIDDEN 128
+int ketgpu_mlp_create(uint64_t seed, ketgpu_mlp** out);
+int ketgpu_mlp_destroy(ketgpu_mlp* m);
+/* Weights as float (W1 128x48, b1 128, W2 128x128, b2 128, w3 128, b3 1). */
+int ketgpu_mlp_get_weights(const ketgpu_mlp* m, float* w1, float* b1, float* w2,
+                           float* b2, float* w3, float* b3);
+int ketgpu_mlp_set_weights(ketgpu_mlp* m, const float* w1, const float* b1,
+                           const float* w2, const float* b2, const float* w3,
+                           const float* b3);
+/* x: batch x 48 host floats -> out: batch predictions. */
+int ketgpu_mlp_forward(ketgpu_mlp* m, const float* x, uint64_t batch, float* out);
+/* Gradients of the mean squared error (host outputs, FP32). */
+int ketgpu_mlp_gradients(ketgpu_mlp* m, const float* x, const float* y,
+                         uint64_t batch, float* loss, float* gw1, float* gb1,
+                         float* gw2, float* gb2, float* gw3, float* gb3);
+/* `steps` Adam steps over (x, y) minibatches drawn by the library. */
+int ketgpu_mlp_train(ketgpu_mlp* m, const float* x, const float* y,
+                     uint64_t n_samples, uint64_t steps, uint64_t minibatch,
+                     float lr, float* final_loss);
+/* Attach a model to the learned planner (NULL detaches). */
+int ketgpu_planner_set_model(ketgpu_mlp* m);
+/* The 48 features the planner scores a candidate block by. */
+int ketgpu_block_features(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
+                          const int32_t* block_qubits, int32_t k, float* out48);
+/* Time one dense k-qubit block pass on a state (microseconds, CUDA events). */
+int ketgpu_time_block(ketgpu_state* s, const int32_t* block_qubits, int32_t k,
+                      int32_t n_gates, int32_t reps, float* out_us);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

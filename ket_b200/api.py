@@ -1,0 +1,422 @@
+"""ket's Python API on the B200 backend (bindings/python/module.cpp:41-271).
+
+Same names and argument meaning as ket's ``_ket`` module -- ``run``,
+``run_with_probes``, ``expval`` (four overloads), ``measure``, ``sample``,
+``is_clifford``, ``chosen_method``, ``set_num_threads``/``num_threads`` --
+with every state-vector computation on the GPU through the C ABI.  Extras
+for large states: ``run_device`` returns a ``DeviceState`` that never leaves
+HBM, and ``set_options`` selects precision (complex128 by default, as ket),
+fusion mode and the tensor-core path.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import threading
+from typing import Iterable, List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+from . import _lib
+from ._lib import C64, C128, FUSE_GREEDY, FUSE_LEARNED, FUSE_NONE, FUSE_REFERENCE, check, lib
+from .circuit import Circuit
+
+_PRECISIONS = {"c64": C64, "complex64": C64, "c128": C128, "complex128": C128}
+_FUSIONS = {"none": FUSE_NONE, "unfused": FUSE_NONE, "reference": FUSE_REFERENCE,
+            "greedy": FUSE_GREEDY, "learned": FUSE_LEARNED}
+
+_opts = _lib.Options(C128, FUSE_GREEDY, 5, 1)
+_num_threads = [1]
+
+
+def set_options(precision=None, fusion=None, max_block_qubits=None, tensor_cores=None):
+    """Backend options for later ``run``/``sample``/``expval`` calls."""
+    if precision is not None:
+        _opts.precision = _PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    if fusion is not None:
+        _opts.fusion = _FUSIONS[fusion] if isinstance(fusion, str) else int(fusion)
+    if max_block_qubits is not None:
+        _opts.max_block_qubits = int(max_block_qubits)
+    if tensor_cores is not None:
+        _opts.tensor_cores = 1 if tensor_cores else 0
+
+
+def get_options() -> dict:
+    inv_p = {C64: "c64", C128: "c128"}
+    inv_f = {FUSE_NONE: "none", FUSE_REFERENCE: "reference", FUSE_GREEDY: "greedy", FUSE_LEARNED: "learned"}
+    return {"precision": inv_p[_opts.precision], "fusion": inv_f[_opts.fusion],
+            "max_block_qubits": _opts.max_block_qubits, "tensor_cores": bool(_opts.tensor_cores)}
+
+
+def make_options(precision="c128", fusion="greedy", max_block_qubits=5, tensor_cores=True) -> _lib.Options:
+    return _lib.Options(_PRECISIONS[precision] if isinstance(precision, str) else int(precision),
+                        _FUSIONS[fusion] if isinstance(fusion, str) else int(fusion),
+                        int(max_block_qubits), 1 if tensor_cores else 0)
+
+
+def set_num_threads(threads: int) -> None:
+    """Accepted for ket compatibility (parallelism.hpp:17); the GPU path
+    sizes its own grids, so the value only changes ``num_threads()``."""
+    if threads < 0:
+        raise ValueError("threads must be non-negative")
+    _num_threads[0] = threads if threads else (os.cpu_count() or 1)
+
+
+def num_threads() -> int:
+    return _num_threads[0]
+
+
+# ---------------------------------------------------------------------------
+class DeviceState:
+    """A 2^n state vector resident in GPU memory (complex64 or complex128)."""
+
+    def __init__(self, n_qubits: int, precision="c128"):
+        p = _PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        h = ct.c_void_p()
+        check(lib.ketgpu_state_create(int(n_qubits), p, ct.byref(h)))
+        self._h = h
+        self.n_qubits = int(n_qubits)
+        self.precision = p
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.ketgpu_state_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return 1 << self.n_qubits
+
+    def reset(self):
+        check(lib.ketgpu_state_reset(self._h))
+
+    def apply(self, circuit: Union[Circuit, np.ndarray], options: Optional[_lib.Options] = None):
+        ops = circuit.to_ops() if isinstance(circuit, Circuit) else np.ascontiguousarray(circuit)
+        opt = options or _lib.Options(self.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores)
+        check(lib.ketgpu_apply(self._h, ops.ctypes.data, len(ops), ct.byref(opt)))
+        return self
+
+    def to_numpy(self, first: int = 0, count: Optional[int] = None) -> np.ndarray:
+        dim = 1 << self.n_qubits
+        count = dim - first if count is None else count
+        out = np.empty(count, dtype=np.complex128)
+        check(lib.ketgpu_state_download(self._h, first, count, out.ctypes.data))
+        return out
+
+    def from_numpy(self, amps: np.ndarray, first: int = 0):
+        a = np.ascontiguousarray(amps, dtype=np.complex128)
+        check(lib.ketgpu_state_upload(self._h, first, len(a), a.ctypes.data))
+        return self
+
+    def __getitem__(self, i: int) -> complex:
+        if not (0 <= i < len(self)):
+            raise IndexError()
+        return complex(self.to_numpy(i, 1)[0])
+
+    def norm(self) -> float:
+        v = ct.c_double()
+        check(lib.ketgpu_norm(self._h, ct.byref(v)))
+        return v.value
+
+    def inner(self, other: "DeviceState") -> complex:
+        re, im = ct.c_double(), ct.c_double()
+        check(lib.ketgpu_inner(self._h, other._h, ct.byref(re), ct.byref(im)))
+        return complex(re.value, im.value)
+
+    def expval(self, obs) -> float:
+        return _expval_dev(self, obs)
+
+    def sample(self, uniforms: np.ndarray) -> np.ndarray:
+        u = np.ascontiguousarray(uniforms, dtype=np.float64)
+        out = np.empty(len(u), dtype=np.uint64)
+        check(lib.ketgpu_sample(self._h, u.ctypes.data, len(u), out.ctypes.data))
+        return out
+
+    def torch_view(self):
+        """Zero-copy torch tensor over the device amplitudes (complex)."""
+        import torch
+        ptr = lib.ketgpu_state_device_ptr(self._h)
+        n = 1 << self.n_qubits
+        dt = torch.complex64 if self.precision == C64 else torch.complex128
+
+        class _CAI:
+            __cuda_array_interface__ = {
+                "shape": (n,), "typestr": "<c8" if self.precision == C64 else "<c16",
+                "data": (ptr, False), "version": 3, "strides": None}
+        return torch.as_tensor(_CAI(), device="cuda").view(dt)
+
+
+class State:
+    """ket.State: 2^n complex128 amplitudes on the host (state.hpp:15-34),
+    keeping the device copy it was produced from for further queries."""
+
+    def __init__(self, amps: np.ndarray, device: Optional[DeviceState] = None):
+        self._amps = np.ascontiguousarray(amps, dtype=np.complex128)
+        self._dev = device
+
+    def __len__(self):
+        return len(self._amps)
+
+    def __getitem__(self, i: int) -> complex:
+        if not (0 <= i < len(self._amps)):
+            raise IndexError()
+        return complex(self._amps[i])
+
+    def __repr__(self):
+        return f"<ket_b200.State size={len(self._amps)}>"
+
+    def to_numpy(self) -> np.ndarray:
+        return self._amps
+
+    @property
+    def n_qubits(self) -> int:
+        return int(len(self._amps)).bit_length() - 1
+
+    def device(self) -> DeviceState:
+        if self._dev is None:
+            d = DeviceState(self.n_qubits, C128)
+            d.from_numpy(self._amps)
+            self._dev = d
+        return self._dev
+
+
+class ProbeRun:
+    def __init__(self, final: State, probes: List[Tuple[str, State]]):
+        self.final = final
+        self.probes = probes
+
+
+# ---------------------------------------------------------------------------
+def run_device(circuit: Circuit, precision=None, options: Optional[_lib.Options] = None) -> DeviceState:
+    """Evolve |0...0> on the GPU and keep the state there."""
+    opt = options or _lib.Options(_opts.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores)
+    if precision is not None:
+        opt.precision = _PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    d = DeviceState(circuit.n_qubits, opt.precision)
+    d.apply(circuit, opt)
+    return d
+
+
+def run(circuit: Circuit) -> State:
+    """ket.run (simulator.hpp:15): the final state as a host State."""
+    d = run_device(circuit)
+    return State(d.to_numpy(), d)
+
+
+def run_with_probes(circuit: Circuit) -> ProbeRun:
+    """ket.run_with_probes (simulator.hpp:24, simulator.cpp:560-565)."""
+    from .circuit import GateType
+    d = DeviceState(circuit.n_qubits, _opts.precision)
+    probes = []
+    segment = Circuit(circuit.n_qubits)
+    for g in circuit.flat_gates():
+        if g.type == GateType.Probe:
+            d.apply(segment)
+            probes.append((g.label, State(d.to_numpy())))
+            segment = Circuit(circuit.n_qubits)
+        else:
+            segment._gates.append(g)
+    d.apply(segment)
+    return ProbeRun(State(d.to_numpy(), d), probes)
+
+
+def _terms(obs) -> List[Tuple[float, str]]:
+    if isinstance(obs, str):
+        return [(1.0, obs)]
+    return [(float(c), str(p)) for c, p in obs]
+
+
+def _expval_dev(d: DeviceState, obs) -> float:
+    if isinstance(obs, str):
+        out = ct.c_double()
+        check(lib.ketgpu_expval(d.handle, obs.encode(), ct.byref(out)))
+        return out.value
+    terms = _terms(obs)
+    coeffs = np.array([c for c, _ in terms], dtype=np.float64)
+    arr, keep = _lib.c_strings([p for _, p in terms])
+    out = ct.c_double()
+    check(lib.ketgpu_expval_sum(d.handle, coeffs.ctypes.data, ct.cast(arr, ct.c_void_p), len(terms),
+                                ct.byref(out)))
+    return out.value
+
+
+def _method(method: str) -> str:
+    if method not in ("auto", "statevector", "stabilizer"):
+        raise ValueError("method must be 'auto', 'statevector', or 'stabilizer'")
+    return method
+
+
+def is_clifford(circuit: Circuit) -> bool:
+    return circuit.is_clifford()
+
+
+def chosen_method(circuit: Circuit) -> str:
+    return "stabilizer" if circuit.is_clifford() else "statevector"
+
+
+def _resolve(circuit: Circuit, method: str) -> str:
+    method = _method(method)
+    if method == "auto":
+        method = chosen_method(circuit)
+    if method == "stabilizer" and not circuit.is_clifford():
+        raise ValueError("stabilizer backend requires a Clifford circuit (it contains a non-Clifford gate); "
+                         "use Method::Auto or Method::StateVector")
+    return method
+
+
+def _stabilizer():
+    """ket's own CPU stabilizer tableau (src/backends/stabilizer.cpp), which
+    this backend leaves untouched: ket's Python module when it is installed."""
+    try:
+        import ket as _ket  # the reference package
+        return _ket
+    except ImportError as e:
+        raise RuntimeError(
+            "Clifford circuits are simulated by ket's own stabilizer tableau; install ket "
+            "(or link the C++ drop-in into ket) to use method='stabilizer'") from e
+
+
+def _to_ket(circuit: Circuit):
+    k = _stabilizer()
+    c = k.Circuit(circuit.n_qubits)
+    from .circuit import GateType as G
+    for g in circuit.flat_gates():
+        name = {G.H: "h", G.X: "x", G.Y: "y", G.Z: "z", G.S: "s", G.Sdg: "sdg", G.CX: "cx",
+                G.CY: "cy", G.CZ: "cz", G.Swap: "swap"}.get(g.type)
+        if name:
+            getattr(c, name)(*g.qubits)
+        elif g.type == G.Measure:
+            c.measure(g.qubits[0], g.clbit)
+        elif g.type == G.Barrier:
+            c.barrier()
+    return c
+
+
+def expval(target, obs, method: str = "auto") -> float:
+    """The four overloads of ket.expval (module.cpp:180-213)."""
+    if isinstance(target, State):
+        return _expval_dev(target.device(), obs)
+    if isinstance(target, DeviceState):
+        return _expval_dev(target, obs)
+    if isinstance(target, Circuit):
+        m = _resolve(target, method)
+        if m == "stabilizer":
+            k = _stabilizer()
+            return k.expval(_to_ket(target), obs if isinstance(obs, str) else list(obs), "stabilizer")
+        d = run_device(target)
+        try:
+            return _expval_dev(d, obs)
+        finally:
+            d.close()
+    raise TypeError("expval: expected a State, DeviceState or Circuit")
+
+
+_tls = threading.local()
+
+
+def _auto_seed() -> int:
+    return int.from_bytes(os.urandom(4), "little")
+
+
+def uniforms(seed: int, count: int) -> np.ndarray:
+    """The draws of uniform_real_distribution<double>(0,1) on std::mt19937{seed}."""
+    out = np.empty(count, dtype=np.float64)
+    check(lib.ketgpu_uniforms_mt19937(int(seed) & 0xFFFFFFFF, count, out.ctypes.data))
+    return out
+
+
+def measure(state, seed: Optional[int] = None) -> int:
+    """ket.measure (module.cpp:242-253): one Born-rule draw."""
+    d = state.device() if isinstance(state, State) else state
+    out = ct.c_uint64()
+    check(lib.ketgpu_measure(d.handle, (_auto_seed() if seed is None else int(seed)) & 0xFFFFFFFF,
+                             ct.byref(out)))
+    return int(out.value)
+
+
+def sample(circuit: Circuit, seed: Optional[int] = None, method: str = "auto") -> List[int]:
+    """ket.sample (module.cpp:255-270): one shot of the circuit's measurements."""
+    m = _resolve(circuit, method)
+    if m == "stabilizer":
+        k = _stabilizer()
+        return list(k.sample(_to_ket(circuit), seed, "stabilizer"))
+    d = run_device(circuit)
+    try:
+        u = uniforms(_auto_seed() if seed is None else int(seed), 1)
+        outcome = int(d.sample(u)[0])
+    finally:
+        d.close()
+    creg = [0] * circuit.n_clbits
+    for q, cb in circuit.measurements():
+        creg[cb] = (outcome >> q) & 1
+    return creg
+
+
+def sample_shots(circuit: Circuit, shots: int, seed: int = 0) -> np.ndarray:
+    """Many shots from one evolution (one CDF), the draws of one
+    std::mt19937{seed} stream in order; returns shots x n_clbits."""
+    d = run_device(circuit)
+    try:
+        outcomes = d.sample(uniforms(seed, shots))
+    finally:
+        d.close()
+    meas = circuit.measurements()
+    creg = np.zeros((shots, circuit.n_clbits), dtype=np.int32)
+    for q, cb in meas:
+        creg[:, cb] = ((outcomes >> np.uint64(q)) & np.uint64(1)).astype(np.int32)
+    return creg
+
+
+def plan_stats(circuit: Circuit, options: Optional[_lib.Options] = None) -> dict:
+    ops = circuit.to_ops()
+    opt = options or _lib.Options(_opts.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores)
+    h = ct.c_void_p()
+    check(lib.ketgpu_plan_create(circuit.n_qubits, ops.ctypes.data, len(ops), ct.byref(opt), ct.byref(h)))
+    st = _lib.PlanStats()
+    try:
+        check(lib.ketgpu_plan_stats_get(h, ct.byref(st)))
+    finally:
+        lib.ketgpu_plan_destroy(h)
+    return {f: getattr(st, f) for f, _ in _lib.PlanStats._fields_}
+
+
+class Plan:
+    """A compiled circuit (fusion blocks, matrices on the device) for repeated runs."""
+
+    def __init__(self, n_qubits: int, ops: np.ndarray, options: _lib.Options):
+        self.n_qubits = n_qubits
+        self._ops = np.ascontiguousarray(ops)
+        h = ct.c_void_p()
+        check(lib.ketgpu_plan_create(n_qubits, self._ops.ctypes.data, len(self._ops), ct.byref(options),
+                                     ct.byref(h)))
+        self._h = h
+
+    def stats(self) -> dict:
+        st = _lib.PlanStats()
+        check(lib.ketgpu_plan_stats_get(self._h, ct.byref(st)))
+        return {f: getattr(st, f) for f, _ in _lib.PlanStats._fields_}
+
+    def execute(self, state: DeviceState, sync: bool = True):
+        check(lib.ketgpu_plan_execute(self._h, state.handle))
+        if sync:
+            check(lib.ketgpu_state_synchronize(state.handle))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.ketgpu_plan_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

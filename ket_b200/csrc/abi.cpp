@@ -1,0 +1,588 @@
+// abi.cpp -- the C ABI of libket_b200.so (declared in include/ket_b200.h).
+//
+// Every entry point converts exceptions into KETGPU_ERR_* codes with a
+// thread-local message, validates its arguments on the host before any
+// launch, and leaves the caller's current CUDA device unchanged.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "internal.h"
+
+#define KB_API extern "C" __attribute__((visibility("default")))
+
+namespace kb {
+
+std::atomic<uint64_t> g_launches{0};
+
+namespace {
+thread_local std::string t_err;
+}
+
+void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  const int code = (e == cudaErrorMemoryAllocation) ? KETGPU_ERR_OOM : KETGPU_ERR_CUDA;
+  throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+DeviceGuard::DeviceGuard(int dev) {
+  KB_CUDA(cudaGetDevice(&prev));
+  if (prev != dev) KB_CUDA(cudaSetDevice(dev));
+}
+DeviceGuard::~DeviceGuard() {
+  int cur = -1;
+  if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) cudaSetDevice(prev);
+}
+
+Plan::~Plan() {
+  if (device >= 0) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    if (d_mat64) cudaFree(d_mat64);
+    if (d_mat32) cudaFree(d_mat32);
+    if (d_tc) cudaFree(d_tc);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+}
+
+void pauli_masks(int n, const char* pauli, uint64_t& flip, uint64_t& sign, int& q) {
+  if (!pauli) fail(KETGPU_ERR_INVALID, "expval: null Pauli string");
+  const size_t len = std::strlen(pauli);
+  if (len != (size_t)n)
+    fail(KETGPU_ERR_INVALID, "expval: Pauli string length must equal the number of qubits");
+  flip = 0;
+  sign = 0;
+  int num_y = 0;
+  for (int i = 0; i < n; ++i) {
+    char p = pauli[n - 1 - i];  // rightmost character acts on qubit 0
+    if (p >= 'a' && p <= 'z') p = (char)(p - ('a' - 'A'));
+    const uint64_t bit = uint64_t{1} << i;
+    switch (p) {
+      case 'I': break;
+      case 'X': flip |= bit; break;
+      case 'Y': flip |= bit; sign |= bit; ++num_y; break;
+      case 'Z': sign |= bit; break;
+      default: fail(KETGPU_ERR_INVALID, std::string("expval: invalid Pauli character '") + p + "'");
+    }
+  }
+  q = num_y % 4;
+}
+
+void upload_plan_matrices(Plan& plan, int device) {
+  if (plan.device == device) return;
+  if (plan.device >= 0) fail(KETGPU_ERR_INVALID, "plan was prepared for another device");
+  plan.device = device;
+  if (plan.matrices.empty()) return;
+  std::vector<double> h64;
+  std::vector<float> h32;
+  std::vector<uint32_t> htc, img;
+  plan.off64.assign(plan.matrices.size(), 0);
+  plan.off32.assign(plan.matrices.size(), 0);
+  plan.offtc.assign(plan.matrices.size(), 0);
+  // matrix index -> whether its pass is on the tensor cores
+  std::vector<int> kof(plan.matrices.size(), 0);
+  std::vector<char> tensor(plan.matrices.size(), 0);
+  for (const Pass& p : plan.passes)
+    if (p.kind == PassKind::Fused) {
+      kof[p.mat_index] = p.k;
+      tensor[p.mat_index] = p.tensor;
+    }
+  for (size_t i = 0; i < plan.matrices.size(); ++i) {
+    const std::vector<cplx>& m = plan.matrices[i];
+    const int dim = 1 << kof[i];
+    if (plan.precision == KETGPU_C128) {
+      plan.off64[i] = h64.size() * sizeof(double);
+      for (int c = 0; c < dim; ++c)
+        for (int r = 0; r < dim; ++r) {
+          h64.push_back(m[(size_t)r * dim + c].real());
+          h64.push_back(m[(size_t)r * dim + c].imag());
+        }
+      while (h64.size() % 2) h64.push_back(0);
+    } else if (tensor[i]) {
+      plan.offtc[i] = htc.size() * sizeof(uint32_t);
+      build_tc_image(m, kof[i], img);
+      htc.insert(htc.end(), img.begin(), img.end());
+      while (htc.size() % 64) htc.push_back(0);  // 256-byte alignment
+    } else {
+      plan.off32[i] = h32.size() * sizeof(float);
+      for (int c = 0; c < dim; ++c)
+        for (int r = 0; r < dim; ++r) {
+          h32.push_back((float)m[(size_t)r * dim + c].real());
+          h32.push_back((float)m[(size_t)r * dim + c].imag());
+        }
+      while (h32.size() % 4) h32.push_back(0);
+    }
+  }
+  if (!h64.empty()) {
+    KB_CUDA(cudaMalloc(&plan.d_mat64, h64.size() * sizeof(double)));
+    KB_CUDA(cudaMemcpy(plan.d_mat64, h64.data(), h64.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (!h32.empty()) {
+    KB_CUDA(cudaMalloc(&plan.d_mat32, h32.size() * sizeof(float)));
+    KB_CUDA(cudaMemcpy(plan.d_mat32, h32.data(), h32.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (!htc.empty()) {
+    KB_CUDA(cudaMalloc(&plan.d_tc, htc.size() * sizeof(uint32_t)));
+    KB_CUDA(cudaMemcpy(plan.d_tc, htc.data(), htc.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  }
+}
+
+int tc_error_flag(bool reset);
+
+namespace {
+
+State* as_state(ketgpu_state* s) { return reinterpret_cast<State*>(s); }
+const State* as_state(const ketgpu_state* s) { return reinterpret_cast<const State*>(s); }
+Plan* as_plan(ketgpu_plan* p) { return reinterpret_cast<Plan*>(p); }
+const Plan* as_plan(const ketgpu_plan* p) { return reinterpret_cast<const Plan*>(p); }
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return KETGPU_OK;
+  } catch (const Error& e) {
+    t_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    t_err = "host allocation failed";
+    return KETGPU_ERR_OOM;
+  } catch (const std::exception& e) {
+    t_err = e.what();
+    return KETGPU_ERR_LOGIC;
+  }
+}
+
+void need(bool cond, const char* msg) {
+  if (!cond) fail(KETGPU_ERR_INVALID, msg);
+}
+
+// Parallel host conversion helpers for the host<->device complex128 copies.
+template <class F>
+void parallel_chunks(uint64_t count, F&& f) {
+  unsigned nt = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  if (count < (1u << 20)) nt = 1;
+  std::vector<std::thread> th;
+  const uint64_t per = (count + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const uint64_t lo = t * per, hi = std::min(count, lo + per);
+    if (lo >= hi) break;
+    th.emplace_back([&, lo, hi] { f(lo, hi); });
+  }
+  for (auto& x : th) x.join();
+}
+
+struct Pinned {
+  void* p = nullptr;
+  explicit Pinned(size_t b) { KB_CUDA(cudaMallocHost(&p, b)); }
+  ~Pinned() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+constexpr uint64_t kChunk = uint64_t{1} << 24;  // amplitudes per staged copy
+
+void download(const State& s, uint64_t first, uint64_t count, double* out) {
+  if (s.precision == KETGPU_C128) {
+    KB_CUDA(cudaMemcpyAsync(out, static_cast<const double2*>(s.amps) + first, count * 16,
+                            cudaMemcpyDeviceToHost, s.stream));
+    KB_CUDA(cudaStreamSynchronize(s.stream));
+    return;
+  }
+  const uint64_t chunk = std::min<uint64_t>(kChunk, std::max<uint64_t>(count, 1));
+  Pinned stage(2 * chunk * 8);
+  float2* buf[2] = {static_cast<float2*>(stage.p), static_cast<float2*>(stage.p) + chunk};
+  cudaEvent_t ev[2];
+  KB_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  KB_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  const uint64_t nchunks = (count + chunk - 1) / chunk;
+  auto issue = [&](uint64_t c) {
+    const uint64_t lo = c * chunk, len = std::min(chunk, count - lo);
+    KB_CUDA(cudaMemcpyAsync(buf[c & 1], static_cast<const float2*>(s.amps) + first + lo, len * 8,
+                            cudaMemcpyDeviceToHost, s.stream));
+    KB_CUDA(cudaEventRecord(ev[c & 1], s.stream));
+  };
+  if (nchunks) issue(0);
+  for (uint64_t c = 0; c < nchunks; ++c) {
+    KB_CUDA(cudaEventSynchronize(ev[c & 1]));
+    if (c + 1 < nchunks) issue(c + 1);
+    const uint64_t lo = c * chunk, len = std::min(chunk, count - lo);
+    const float2* src = buf[c & 1];
+    double* dst = out + 2 * lo;
+    parallel_chunks(len, [&](uint64_t a, uint64_t b) {
+      for (uint64_t i = a; i < b; ++i) {
+        dst[2 * i] = (double)src[i].x;
+        dst[2 * i + 1] = (double)src[i].y;
+      }
+    });
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+}
+
+void upload(State& s, uint64_t first, uint64_t count, const double* in) {
+  if (s.precision == KETGPU_C128) {
+    KB_CUDA(cudaMemcpyAsync(static_cast<double2*>(s.amps) + first, in, count * 16, cudaMemcpyHostToDevice,
+                            s.stream));
+    KB_CUDA(cudaStreamSynchronize(s.stream));
+    return;
+  }
+  const uint64_t chunk = std::min<uint64_t>(kChunk, std::max<uint64_t>(count, 1));
+  Pinned stage(chunk * 8);
+  float2* buf = static_cast<float2*>(stage.p);
+  for (uint64_t lo = 0; lo < count; lo += chunk) {
+    const uint64_t len = std::min(chunk, count - lo);
+    parallel_chunks(len, [&](uint64_t a, uint64_t b) {
+      for (uint64_t i = a; i < b; ++i) buf[i] = make_float2((float)in[2 * (lo + i)], (float)in[2 * (lo + i) + 1]);
+    });
+    KB_CUDA(cudaMemcpyAsync(static_cast<float2*>(s.amps) + first + lo, buf, len * 8, cudaMemcpyHostToDevice,
+                            s.stream));
+    KB_CUDA(cudaStreamSynchronize(s.stream));
+  }
+}
+
+void execute(const Plan& plan, State& s) {
+  need(plan.n == s.n, "plan and state have different qubit counts");
+  need(plan.precision == s.precision, "plan and state have different precisions");
+  upload_plan_matrices(const_cast<Plan&>(plan), s.device);
+  for (const Pass& p : plan.passes) launch_pass(s, plan, p);
+}
+
+void check_tc_flag() {
+  if (tc_error_flag(true))
+    fail(KETGPU_ERR_TIMEOUT, "tensor-core block kernel timed out waiting on its MMA barrier");
+}
+
+}  // namespace
+
+// Create a state on the current device (used by adjoint.cu too).
+State* create_state(int n, int precision) {
+  if (n < 0 || n > 40) fail(KETGPU_ERR_INVALID, "n_qubits must be in [0, 40]");
+  if (precision != KETGPU_C64 && precision != KETGPU_C128)
+    fail(KETGPU_ERR_INVALID, "precision must be KETGPU_C64 or KETGPU_C128");
+  auto st = std::make_unique<State>();
+  st->n = n;
+  st->precision = precision;
+  KB_CUDA(cudaGetDevice(&st->device));
+  const size_t bytes = (size_t)st->dim() * st->amp_bytes();
+  size_t free_b = 0, total_b = 0;
+  KB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  if (bytes > free_b)
+    fail(KETGPU_ERR_OOM, "state of " + std::to_string(bytes) + " bytes exceeds free device memory (" +
+                             std::to_string(free_b) + ")");
+  KB_CUDA(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking));
+  const cudaError_t e = cudaMalloc(&st->amps, bytes);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(st->stream);
+    check_cuda(e, "cudaMalloc(state)");
+  }
+  set_ground(*st);
+  return st.release();
+}
+
+void destroy_state(State* s) {
+  if (!s) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->amps) cudaFree(s->amps);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete s;
+}
+
+void execute_plan(const Plan& plan, State& s) { execute(plan, s); }
+
+}  // namespace kb
+
+using namespace kb;
+
+KB_API const char* ketgpu_last_error(void) { return t_err.c_str(); }
+KB_API int ketgpu_abi_version(void) { return KETGPU_ABI_VERSION; }
+KB_API uint64_t ketgpu_launch_count(void) { return g_launches.load(); }
+
+KB_API int ketgpu_state_create(int32_t n_qubits, int32_t precision, ketgpu_state** out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    *out = reinterpret_cast<ketgpu_state*>(create_state(n_qubits, precision));
+  });
+}
+
+KB_API int ketgpu_state_destroy(ketgpu_state* s) {
+  return guard([&] { destroy_state(as_state(s)); });
+}
+
+KB_API int ketgpu_state_reset(ketgpu_state* s) {
+  return guard([&] {
+    need(s != nullptr, "state is null");
+    DeviceGuard g(as_state(s)->device);
+    set_ground(*as_state(s));
+    KB_CUDA(cudaStreamSynchronize(as_state(s)->stream));
+  });
+}
+
+KB_API int ketgpu_state_info(const ketgpu_state* s, int32_t* n, int32_t* precision) {
+  return guard([&] {
+    need(s != nullptr, "state is null");
+    if (n) *n = as_state(s)->n;
+    if (precision) *precision = as_state(s)->precision;
+  });
+}
+
+KB_API void* ketgpu_state_device_ptr(const ketgpu_state* s) { return s ? as_state(s)->amps : nullptr; }
+
+KB_API int ketgpu_state_download(const ketgpu_state* s, uint64_t first, uint64_t count, double* out) {
+  return guard([&] {
+    need(s != nullptr && (out != nullptr || count == 0), "null argument");
+    const State& st = *as_state(s);
+    if (first > st.dim() || count > st.dim() - first)
+      fail(KETGPU_ERR_OUT_OF_RANGE, "amplitude range outside the state");
+    DeviceGuard g(st.device);
+    download(st, first, count, out);
+  });
+}
+
+KB_API int ketgpu_state_upload(ketgpu_state* s, uint64_t first, uint64_t count, const double* in) {
+  return guard([&] {
+    need(s != nullptr && (in != nullptr || count == 0), "null argument");
+    State& st = *as_state(s);
+    if (first > st.dim() || count > st.dim() - first)
+      fail(KETGPU_ERR_OUT_OF_RANGE, "amplitude range outside the state");
+    DeviceGuard g(st.device);
+    upload(st, first, count, in);
+  });
+}
+
+KB_API int ketgpu_state_copy(const ketgpu_state* src, ketgpu_state* dst) {
+  return guard([&] {
+    need(src && dst, "null state");
+    const State& a = *as_state(src);
+    State& b = *as_state(dst);
+    need(a.n == b.n && a.precision == b.precision, "states differ in size or precision");
+    DeviceGuard g(b.device);
+    KB_CUDA(cudaStreamSynchronize(a.stream));
+    KB_CUDA(cudaMemcpyAsync(b.amps, a.amps, a.dim() * a.amp_bytes(), cudaMemcpyDefault, b.stream));
+    KB_CUDA(cudaStreamSynchronize(b.stream));
+  });
+}
+
+KB_API int ketgpu_state_synchronize(ketgpu_state* s) {
+  return guard([&] {
+    need(s != nullptr, "state is null");
+    DeviceGuard g(as_state(s)->device);
+    KB_CUDA(cudaStreamSynchronize(as_state(s)->stream));
+    check_tc_flag();
+  });
+}
+
+KB_API int ketgpu_plan_create(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const ketgpu_options* opt,
+                              ketgpu_plan** out) {
+  return guard([&] {
+    need(out != nullptr, "out is null");
+    need(ops != nullptr || n_ops == 0, "ops is null");
+    if (n < 0 || n > 40) fail(KETGPU_ERR_INVALID, "n_qubits must be in [0, 40]");
+    validate_ops(n, ops, n_ops);
+    auto plan = std::make_unique<Plan>();
+    build_plan(*plan, n, ops, n_ops, resolve_options(opt));
+    *out = reinterpret_cast<ketgpu_plan*>(plan.release());
+  });
+}
+
+KB_API int ketgpu_plan_destroy(ketgpu_plan* p) {
+  return guard([&] { delete as_plan(p); });
+}
+
+KB_API int ketgpu_plan_stats_get(const ketgpu_plan* p, ketgpu_plan_stats* out) {
+  return guard([&] {
+    need(p && out, "null argument");
+    *out = as_plan(p)->stats;
+  });
+}
+
+KB_API int ketgpu_plan_execute(const ketgpu_plan* p, ketgpu_state* s) {
+  return guard([&] {
+    need(p && s, "null argument");
+    DeviceGuard g(as_state(s)->device);
+    execute(*as_plan(p), *as_state(s));
+  });
+}
+
+KB_API int ketgpu_apply(ketgpu_state* s, const ketgpu_op* ops, uint64_t n_ops, const ketgpu_options* opt) {
+  return guard([&] {
+    need(s != nullptr, "state is null");
+    need(ops != nullptr || n_ops == 0, "ops is null");
+    State& st = *as_state(s);
+    validate_ops(st.n, ops, n_ops);
+    PlanOptions o = resolve_options(opt);
+    if (opt == nullptr) o.precision = st.precision;
+    need(o.precision == st.precision, "options precision differs from the state's");
+    Plan plan;
+    build_plan(plan, st.n, ops, n_ops, o);
+    DeviceGuard g(st.device);
+    execute(plan, st);
+    KB_CUDA(cudaStreamSynchronize(st.stream));
+    check_tc_flag();
+  });
+}
+
+KB_API int ketgpu_run(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const ketgpu_options* opt,
+                      double* out_c128) {
+  return guard([&] {
+    need(out_c128 != nullptr, "out is null");
+    need(ops != nullptr || n_ops == 0, "ops is null");
+    if (n < 0 || n > 40) fail(KETGPU_ERR_INVALID, "n_qubits must be in [0, 40]");
+    validate_ops(n, ops, n_ops);
+    const PlanOptions o = resolve_options(opt);
+    Plan plan;
+    build_plan(plan, n, ops, n_ops, o);
+    std::unique_ptr<State, void (*)(State*)> st(create_state(n, o.precision), destroy_state);
+    execute(plan, *st);
+    download(*st, 0, st->dim(), out_c128);
+    check_tc_flag();
+  });
+}
+
+KB_API int ketgpu_norm(const ketgpu_state* s, double* out) {
+  return guard([&] {
+    need(s && out, "null argument");
+    DeviceGuard g(as_state(s)->device);
+    *out = reduce_norm(*as_state(s));
+  });
+}
+
+KB_API int ketgpu_inner(const ketgpu_state* a, const ketgpu_state* b, double* re, double* im) {
+  return guard([&] {
+    need(a && b, "null state");
+    need(as_state(a)->n == as_state(b)->n && as_state(a)->precision == as_state(b)->precision,
+         "states differ in size or precision");
+    DeviceGuard g(as_state(a)->device);
+    const cplx v = reduce_inner(*as_state(a), *as_state(b));
+    if (re) *re = v.real();
+    if (im) *im = v.imag();
+  });
+}
+
+KB_API int ketgpu_expval_terms(const ketgpu_state* s, const char* const* paulis, uint64_t n_terms, double* out) {
+  return guard([&] {
+    need(s != nullptr, "state is null");
+    need((paulis && out) || n_terms == 0, "null argument");
+    const State& st = *as_state(s);
+    std::vector<uint64_t> flip(n_terms), sign(n_terms);
+    std::vector<int> q(n_terms);
+    for (uint64_t t = 0; t < n_terms; ++t) pauli_masks(st.n, paulis[t], flip[t], sign[t], q[t]);
+    DeviceGuard g(st.device);
+    expval_terms(st, flip, sign, q, out);
+  });
+}
+
+KB_API int ketgpu_expval(const ketgpu_state* s, const char* pauli, double* out) {
+  return guard([&] {
+    need(s && out, "null argument");
+    const State& st = *as_state(s);
+    std::vector<uint64_t> flip(1), sign(1);
+    std::vector<int> q(1);
+    pauli_masks(st.n, pauli, flip[0], sign[0], q[0]);
+    DeviceGuard g(st.device);
+    expval_terms(st, flip, sign, q, out);
+  });
+}
+
+KB_API int ketgpu_expval_sum(const ketgpu_state* s, const double* coeffs, const char* const* paulis,
+                             uint64_t n_terms, double* out) {
+  return guard([&] {
+    need(s && out, "null argument");
+    need((coeffs && paulis) || n_terms == 0, "null argument");
+    const State& st = *as_state(s);
+    std::vector<uint64_t> flip(n_terms), sign(n_terms);
+    std::vector<int> q(n_terms);
+    for (uint64_t t = 0; t < n_terms; ++t) pauli_masks(st.n, paulis[t], flip[t], sign[t], q[t]);
+    std::vector<double> per(n_terms);
+    DeviceGuard g(st.device);
+    expval_terms(st, flip, sign, q, per.data());
+    double total = 0.0;  // coefficient-weighted, in term order (observable.cpp:85-91)
+    for (uint64_t t = 0; t < n_terms; ++t) total += coeffs[t] * per[t];
+    *out = total;
+  });
+}
+
+KB_API int ketgpu_uniforms_mt19937(uint32_t seed, uint64_t count, double* out) {
+  return guard([&] {
+    need(out != nullptr || count == 0, "out is null");
+    std::mt19937 rng{seed};
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    for (uint64_t i = 0; i < count; ++i) out[i] = dist(rng);
+  });
+}
+
+KB_API int ketgpu_sample(const ketgpu_state* s, const double* u, uint64_t count, uint64_t* out) {
+  return guard([&] {
+    need(s != nullptr, "state is null");
+    need((u && out) || count == 0, "null argument");
+    DeviceGuard g(as_state(s)->device);
+    sample_tree(*as_state(s), u, count, out);
+  });
+}
+
+KB_API int ketgpu_measure(const ketgpu_state* s, uint32_t seed, uint64_t* out) {
+  return guard([&] {
+    need(s && out, "null argument");
+    std::mt19937 rng{seed};
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    const double u = dist(rng);
+    DeviceGuard g(as_state(s)->device);
+    sample_tree(*as_state(s), &u, 1, out);
+  });
+}
+
+KB_API int ketgpu_plan_execute_timed(const ketgpu_plan* p, ketgpu_state* s, float* pass_ms) {
+  return guard([&] {
+    need(p && s && pass_ms, "null argument");
+    const Plan& plan = *as_plan(p);
+    State& st = *as_state(s);
+    need(plan.n == st.n && plan.precision == st.precision, "plan and state do not match");
+    DeviceGuard g(st.device);
+    upload_plan_matrices(const_cast<Plan&>(plan), st.device);
+    const size_t np = plan.passes.size();
+    std::vector<cudaEvent_t> ev(np + 1);
+    for (auto& e : ev) KB_CUDA(cudaEventCreate(&e));
+    KB_CUDA(cudaEventRecord(ev[0], st.stream));
+    for (size_t i = 0; i < np; ++i) {
+      launch_pass(st, plan, plan.passes[i]);
+      KB_CUDA(cudaEventRecord(ev[i + 1], st.stream));
+    }
+    KB_CUDA(cudaEventSynchronize(ev[np]));
+    for (size_t i = 0; i < np; ++i) KB_CUDA(cudaEventElapsedTime(&pass_ms[i], ev[i], ev[i + 1]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    check_tc_flag();
+  });
+}
+
+KB_API int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* kind, int32_t* k,
+                                 int32_t* tensor, double* bytes) {
+  return guard([&] {
+    need(p != nullptr, "plan is null");
+    const Plan& plan = *as_plan(p);
+    if (index >= plan.passes.size()) fail(KETGPU_ERR_OUT_OF_RANGE, "pass index out of range");
+    const Pass& ps = plan.passes[index];
+    if (kind) *kind = ps.kind == PassKind::Pair ? 0 : ps.kind == PassKind::Phase ? 1 : 2;
+    if (k) *k = ps.kind == PassKind::Fused ? ps.k : ps.nfixed;
+    if (tensor) *tensor = ps.tensor ? 1 : 0;
+    if (bytes) *bytes = ps.bytes(plan.n, plan.precision == KETGPU_C64 ? 8 : 16);
+  });
+}
+
+KB_API void* ketgpu_state_stream(const ketgpu_state* s) {
+  return s ? reinterpret_cast<void*>(as_state(s)->stream) : nullptr;
+}

@@ -1,0 +1,145 @@
+// internal.h -- shared host-side declarations of the B200 state-vector
+// backend (not installed; the public surface is include/ket_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <complex>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ket_b200.h"
+
+namespace kb {
+
+using cplx = std::complex<double>;
+
+// ---- errors ----------------------------------------------------------------
+// Thrown inside the library, turned into KETGPU_ERR_* at the ABI boundary.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] void fail(int code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+#define KB_CUDA(x) ::kb::check_cuda((x), #x)
+
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+// Switch to a device for the lifetime of the guard.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev);
+  ~DeviceGuard();
+};
+
+// ---- state -----------------------------------------------------------------
+struct State {
+  int n = 0;
+  int precision = KETGPU_C64;
+  int device = 0;
+  void* amps = nullptr;  // float2[2^n] or double2[2^n]
+  cudaStream_t stream = nullptr;
+  uint64_t dim() const { return uint64_t{1} << n; }
+  size_t amp_bytes() const { return precision == KETGPU_C64 ? 8 : 16; }
+};
+
+// ---- passes ----------------------------------------------------------------
+// One kernel launch of a plan.
+enum class PassKind : int {
+  Pair,      // 2x2 on (k0, k1) = (base|P0, base|P1), base ranges over the
+             // indices with zeros at the fixed positions
+  Phase,     // multiply the amplitudes with all fixed bits set by a phase
+  Fused,     // dense 2^k x 2^k complex matrix on k qubits
+};
+enum PairMode : int { kPairGeneral = 0, kPairSwap = 1, kPairDiag = 2 };
+
+struct Pass {
+  PassKind kind = PassKind::Pair;
+  int mode = kPairGeneral;
+  int nfixed = 0;
+  int fixed[3] = {0, 0, 0};  // sorted ascending
+  uint64_t p0 = 0, p1 = 0;   // bit patterns of element 0 / element 1
+  cplx m[4];                 // 2x2 (Pair) ; m[0] = phase (Phase)
+  // Fused
+  int k = 0;
+  int qubits[6] = {0, 0, 0, 0, 0, 0};  // sorted ascending; matrix bit b <-> qubits[b]
+  size_t mat_index = 0;                // into Plan::matrices
+  bool tensor = false;                 // tcgen05 path
+  int first_op = 0, n_gates = 0;       // provenance
+  double bytes(int n, size_t amp) const;
+};
+
+struct Plan {
+  int n = 0;
+  int precision = KETGPU_C64;
+  std::vector<Pass> passes;
+  std::vector<std::vector<cplx>> matrices;  // FP64 block matrices (host)
+  // device copies, built lazily per device: FP64 (c128 SIMT), FP32 (c64 SIMT),
+  // tcgen05 B operands (hi/lo TF32 images in the shared-memory layout)
+  void* d_mat64 = nullptr;
+  void* d_mat32 = nullptr;
+  void* d_tc = nullptr;
+  std::vector<size_t> off64, off32, offtc;
+  int device = -1;
+  ketgpu_plan_stats stats{};
+  ~Plan();
+};
+
+// ---- gate lowering -----------------------------------------------------------
+bool is_unitary(int type);
+int gate_arity(int type);
+void validate_ops(int n, const ketgpu_op* ops, uint64_t nops);
+// The 2x2 matrix of a 1-qubit gate (or the target block of a controlled
+// rotation), built with ket's formulas (simulator.cpp:38-97, 166-200).
+void single_matrix(int type, const double* p, cplx m[4]);
+// Lower one gate to its specialised pass.
+Pass lower_gate(const ketgpu_op& op);
+// Per-gate cost in state passes (fraction of the state each pass moves).
+double gate_traffic_fraction(const ketgpu_op& op);
+// Dense block matrix of a gate list restricted to `qubits` (bit b <-> qubits[b]).
+std::vector<cplx> block_matrix(const std::vector<const ketgpu_op*>& gates,
+                               const int* qubits, int k);
+
+// ---- planner ---------------------------------------------------------------
+struct PlanOptions {
+  int precision = KETGPU_C64;
+  int fusion = KETGPU_FUSE_GREEDY;
+  int max_k = 5;
+  bool tensor = true;
+};
+PlanOptions resolve_options(const ketgpu_options* opt);
+void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops,
+                const PlanOptions& o);
+// Learned-planner hook (mlp.cu): score of a candidate block, microseconds.
+bool learned_model_attached();
+float learned_block_cost(int n, const std::vector<const ketgpu_op*>& gates,
+                         const int* qubits, int k);
+void block_features(int n, const std::vector<const ketgpu_op*>& gates,
+                    const int* qubits, int k, float* out48);
+
+// ---- kernel launchers (gates.cu / fused_tc.cu / reduce.cu) -----------------
+void launch_pass(const State& s, const Plan& plan, const Pass& p);
+void upload_plan_matrices(Plan& plan, int device);
+void launch_fused_tc(const State& s, const Pass& p, const void* b_image);
+// Size in bytes of one tcgen05 B image for a k-qubit block.
+size_t tc_image_bytes(int k);
+void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& out);
+bool tc_supported(int k);
+
+void set_ground(const State& s);
+double reduce_norm(const State& s);
+cplx reduce_inner(const State& a, const State& b);
+void expval_terms(const State& s, const std::vector<uint64_t>& flip,
+                  const std::vector<uint64_t>& sign, const std::vector<int>& phase,
+                  double* out);
+void sample_tree(const State& s, const double* u, uint64_t count, uint64_t* out);
+
+// Pauli-string masks (observable.cpp:68-113); throws Error(INVALID).
+void pauli_masks(int n, const char* pauli, uint64_t& flip, uint64_t& sign, int& phase_q);
+
+}  // namespace kb

@@ -1,0 +1,452 @@
+// planner.cpp -- gate lowering and the fusion planner (host, C++20).
+//
+// Lowering follows ket's gate definitions (src/simulator.cpp:38-254 for the
+// matrices, :259-338 for the dispatch).  Planning replaces ket's Fuser
+// (src/simulator.cpp:400-477):
+//   * FUSE_NONE       one specialised kernel per gate (the plain method);
+//   * FUSE_REFERENCE  ket's own rule -- a gate joins the open block only if
+//                     its qubits are a subset of the block's first gate's;
+//   * FUSE_GREEDY     blocks of up to k qubits grown over the gate DAG (a
+//                     gate may join past gates on other qubits, never past a
+//                     pending gate on one of its own qubits), kept only when a
+//                     static byte model says one dense pass beats the
+//                     specialised kernels it replaces;
+//   * FUSE_LEARNED    the same candidate generator, with block costs from the
+//                     MLP cost model and the partition chosen by predicted time.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace kb {
+
+bool is_unitary(int type) { return type >= KETGPU_H && type <= KETGPU_CSWAP; }
+
+int gate_arity(int type) {
+  if (type < 0) return -1;
+  if (type <= KETGPU_U) return 1;
+  if (type <= KETGPU_SWAP) return 2;
+  if (type <= KETGPU_CSWAP) return 3;
+  return 0;
+}
+
+void validate_ops(int n, const ketgpu_op* ops, uint64_t nops) {
+  for (uint64_t i = 0; i < nops; ++i) {
+    const ketgpu_op& o = ops[i];
+    if (o.type < 0 || o.type > KETGPU_PROBE)
+      fail(KETGPU_ERR_INVALID, "ket: unknown gate code " + std::to_string(o.type));
+    if (o.type == KETGPU_COMPOSITE)
+      fail(KETGPU_ERR_INVALID, "ket: composite blocks must be flattened before the device call");
+    const int a = is_unitary(o.type) ? gate_arity(o.type) : (o.type == KETGPU_MEASURE ? 1 : 0);
+    for (int j = 0; j < a; ++j) {
+      if (o.q[j] < 0 || o.q[j] >= n)
+        fail(KETGPU_ERR_OUT_OF_RANGE, "ket: qubit index " + std::to_string(o.q[j]) +
+                                          " is out of range for a " + std::to_string(n) +
+                                          "-qubit circuit");
+      for (int k = 0; k < j; ++k)
+        if (o.q[j] == o.q[k])
+          fail(KETGPU_ERR_INVALID,
+               "ket: a gate cannot act on qubit " + std::to_string(o.q[j]) + " more than once");
+    }
+  }
+}
+
+void single_matrix(int type, const double* p, cplx m[4]) {
+  const double r = 1.0 / std::sqrt(2.0);
+  double c = 0, sn = 0;
+  if (type == KETGPU_RX || type == KETGPU_RY || type == KETGPU_RZ || type == KETGPU_U ||
+      type == KETGPU_CRX || type == KETGPU_CRY || type == KETGPU_CRZ || type == KETGPU_CU) {
+    c = std::cos(p[0] / 2.0);
+    sn = std::sin(p[0] / 2.0);
+  }
+  switch (type) {
+    case KETGPU_H: case KETGPU_CH: m[0] = r; m[1] = r; m[2] = r; m[3] = -r; return;
+    case KETGPU_X: case KETGPU_CX: case KETGPU_CCX: m[0] = 0; m[1] = 1; m[2] = 1; m[3] = 0; return;
+    case KETGPU_Y: case KETGPU_CY: m[0] = 0; m[1] = cplx(0, -1); m[2] = cplx(0, 1); m[3] = 0; return;
+    case KETGPU_Z: m[0] = 1; m[1] = 0; m[2] = 0; m[3] = -1; return;
+    case KETGPU_S: m[0] = 1; m[1] = 0; m[2] = 0; m[3] = cplx(0, 1); return;
+    case KETGPU_SDG: m[0] = 1; m[1] = 0; m[2] = 0; m[3] = cplx(0, -1); return;
+    case KETGPU_T: m[0] = 1; m[1] = 0; m[2] = 0; m[3] = cplx(r, r); return;
+    case KETGPU_TDG: m[0] = 1; m[1] = 0; m[2] = 0; m[3] = cplx(r, -r); return;
+    case KETGPU_RX: case KETGPU_CRX:
+      m[0] = c; m[1] = cplx(0, -sn); m[2] = cplx(0, -sn); m[3] = c; return;
+    case KETGPU_RY: case KETGPU_CRY: m[0] = c; m[1] = -sn; m[2] = sn; m[3] = c; return;
+    case KETGPU_RZ: case KETGPU_CRZ: m[0] = cplx(c, -sn); m[1] = 0; m[2] = 0; m[3] = cplx(c, sn); return;
+    case KETGPU_U: case KETGPU_CU:
+      m[0] = cplx(c, 0.0);
+      m[1] = -std::polar(sn, p[2]);
+      m[2] = std::polar(sn, p[1]);
+      m[3] = std::polar(c, p[1] + p[2]);
+      return;
+    default:
+      fail(KETGPU_ERR_LOGIC, "single_matrix: not a 1-qubit gate");
+  }
+}
+
+namespace {
+
+void set_fixed(Pass& p, std::initializer_list<int> qs) {
+  p.nfixed = 0;
+  for (int q : qs) p.fixed[p.nfixed++] = q;
+  std::sort(p.fixed, p.fixed + p.nfixed);
+}
+
+}  // namespace
+
+Pass lower_gate(const ketgpu_op& op) {
+  Pass p;
+  const int t = op.type;
+  const auto bit = [&](int j) { return uint64_t{1} << op.q[j]; };
+  if (gate_arity(t) == 1) {
+    single_matrix(t, op.p, p.m);
+    if (t == KETGPU_Z || t == KETGPU_S || t == KETGPU_SDG || t == KETGPU_T || t == KETGPU_TDG) {
+      p.kind = PassKind::Phase;
+      set_fixed(p, {op.q[0]});
+      p.p0 = bit(0);
+      p.m[0] = p.m[3];
+    } else {
+      p.kind = PassKind::Pair;
+      set_fixed(p, {op.q[0]});
+      p.p0 = 0;
+      p.p1 = bit(0);
+      p.mode = (t == KETGPU_X) ? kPairSwap : (t == KETGPU_RZ) ? kPairDiag : kPairGeneral;
+    }
+    return p;
+  }
+  switch (t) {
+    case KETGPU_CZ: case KETGPU_CP:
+      p.kind = PassKind::Phase;
+      set_fixed(p, {op.q[0], op.q[1]});
+      p.p0 = bit(0) | bit(1);
+      p.m[0] = (t == KETGPU_CZ) ? cplx(-1.0, 0.0) : cplx(std::cos(op.p[0]), std::sin(op.p[0]));
+      return p;
+    case KETGPU_SWAP:
+      p.kind = PassKind::Pair;
+      p.mode = kPairSwap;
+      set_fixed(p, {op.q[0], op.q[1]});
+      p.p0 = bit(0);
+      p.p1 = bit(1);
+      return p;
+    case KETGPU_CCX:
+      p.kind = PassKind::Pair;
+      p.mode = kPairSwap;
+      set_fixed(p, {op.q[0], op.q[1], op.q[2]});
+      p.p0 = bit(0) | bit(1);
+      p.p1 = bit(0) | bit(1) | bit(2);
+      return p;
+    case KETGPU_CSWAP:
+      p.kind = PassKind::Pair;
+      p.mode = kPairSwap;
+      set_fixed(p, {op.q[0], op.q[1], op.q[2]});
+      p.p0 = bit(0) | bit(1);
+      p.p1 = bit(0) | bit(2);
+      return p;
+    default: {  // controlled 2x2: CH, CX, CY, CRx, CRy, CRz, CU
+      single_matrix(t, op.p, p.m);
+      p.kind = PassKind::Pair;
+      p.mode = (t == KETGPU_CX) ? kPairSwap : (t == KETGPU_CRZ) ? kPairDiag : kPairGeneral;
+      set_fixed(p, {op.q[0], op.q[1]});
+      p.p0 = bit(0);
+      p.p1 = bit(0) | bit(1);
+      return p;
+    }
+  }
+}
+
+double gate_traffic_fraction(const ketgpu_op& op) {
+  const Pass p = lower_gate(op);
+  if (p.kind == PassKind::Phase) return std::ldexp(1.0, -p.nfixed);
+  return std::ldexp(1.0, 1 - p.nfixed);
+}
+
+namespace {
+
+// Apply a lowered pass to a small dense vector (host, FP64).
+void apply_small(const Pass& p, cplx* v, int nloc) {
+  const uint64_t dim = uint64_t{1} << nloc;
+  const uint64_t count = dim >> p.nfixed;
+  for (uint64_t i = 0; i < count; ++i) {
+    uint64_t b = i;
+    for (int j = 0; j < p.nfixed; ++j) {
+      const int f = p.fixed[j];
+      b = ((b >> f) << (f + 1)) | (b & ((uint64_t{1} << f) - 1));
+    }
+    if (p.kind == PassKind::Phase) {
+      v[b | p.p0] *= p.m[0];
+      continue;
+    }
+    const cplx a = v[b | p.p0], c = v[b | p.p1];
+    if (p.mode == kPairSwap) {
+      v[b | p.p0] = c;
+      v[b | p.p1] = a;
+    } else {
+      v[b | p.p0] = p.m[0] * a + p.m[1] * c;
+      v[b | p.p1] = p.m[2] * a + p.m[3] * c;
+    }
+  }
+}
+
+}  // namespace
+
+std::vector<cplx> block_matrix(const std::vector<const ketgpu_op*>& gates, const int* qubits, int k) {
+  const int dim = 1 << k;
+  std::vector<Pass> local;
+  local.reserve(gates.size());
+  for (const ketgpu_op* g : gates) {
+    ketgpu_op o = *g;
+    for (int j = 0; j < gate_arity(o.type); ++j) {
+      int li = -1;
+      for (int b = 0; b < k; ++b)
+        if (qubits[b] == o.q[j]) li = b;
+      if (li < 0) fail(KETGPU_ERR_LOGIC, "block_matrix: gate outside block");
+      o.q[j] = li;
+    }
+    local.push_back(lower_gate(o));
+  }
+  std::vector<cplx> mat((size_t)dim * dim);
+  std::vector<cplx> col(dim);
+  for (int c = 0; c < dim; ++c) {
+    std::fill(col.begin(), col.end(), cplx(0.0, 0.0));
+    col[c] = 1.0;
+    for (const Pass& p : local) apply_small(p, col.data(), k);
+    for (int r = 0; r < dim; ++r) mat[(size_t)r * dim + c] = col[r];
+  }
+  return mat;
+}
+
+PlanOptions resolve_options(const ketgpu_options* opt) {
+  PlanOptions o;
+  if (!opt) return o;
+  if (opt->precision != KETGPU_C64 && opt->precision != KETGPU_C128)
+    fail(KETGPU_ERR_INVALID, "precision must be KETGPU_C64 or KETGPU_C128");
+  if (opt->fusion < KETGPU_FUSE_NONE || opt->fusion > KETGPU_FUSE_LEARNED)
+    fail(KETGPU_ERR_INVALID, "unknown fusion mode");
+  o.precision = opt->precision;
+  o.fusion = opt->fusion;
+  o.max_k = opt->max_block_qubits ? opt->max_block_qubits : 5;
+  if (o.max_k < 1 || o.max_k > 6) fail(KETGPU_ERR_INVALID, "max_block_qubits must be in [1, 6]");
+  o.tensor = opt->tensor_cores != 0;
+  return o;
+}
+
+namespace {
+
+struct Block {
+  std::vector<int> gates;  // op indices, program order
+  std::vector<int> qubits; // sorted
+};
+
+// Cost (in full-state passes) of a dense k-qubit block pass: one HBM pass,
+// plus the compute that outgrows it at large k.
+double fused_cost_static(int k, int precision, bool tensor) {
+  if (precision == KETGPU_C128) return k <= 4 ? 1.0 : (k == 5 ? 1.35 : 2.7);
+  if (tensor && (k == 4 || k == 5)) return 1.0;
+  return k <= 4 ? 1.0 : (k == 5 ? 1.45 : 2.9);
+}
+
+// Greedy DAG-aware block growth over gates [lo, hi) of `ops`.
+std::vector<Block> grow_blocks(int n, const ketgpu_op* ops, const std::vector<int>& order, int max_k) {
+  std::vector<Block> blocks;
+  std::vector<char> done(order.size(), 0);
+  size_t first = 0;
+  std::vector<char> blocked(n, 0), inq(n, 0);
+  while (true) {
+    while (first < order.size() && done[first]) ++first;
+    if (first == order.size()) break;
+    Block b;
+    std::fill(blocked.begin(), blocked.end(), 0);
+    std::fill(inq.begin(), inq.end(), 0);
+    int nq = 0, nblocked = 0;
+    for (size_t i = first; i < order.size(); ++i) {
+      if (done[i]) continue;
+      const ketgpu_op& o = ops[order[i]];
+      const int a = gate_arity(o.type);
+      bool hit = false;
+      int add = 0;
+      for (int j = 0; j < a; ++j) {
+        if (blocked[o.q[j]]) hit = true;
+        if (!inq[o.q[j]]) ++add;
+      }
+      if (b.gates.empty() || (!hit && nq + add <= max_k)) {
+        for (int j = 0; j < a; ++j)
+          if (!inq[o.q[j]]) {
+            inq[o.q[j]] = 1;
+            ++nq;
+          }
+        b.gates.push_back((int)i);
+        done[i] = 1;
+      } else {
+        for (int j = 0; j < a; ++j)
+          if (!blocked[o.q[j]]) {
+            blocked[o.q[j]] = 1;
+            ++nblocked;
+          }
+        if (nblocked == n) break;
+        // nothing more can join once every block qubit is blocked and the
+        // block is full
+        if (nq == max_k) {
+          bool open = false;
+          for (int q = 0; q < n; ++q)
+            if (inq[q] && !blocked[q]) open = true;
+          if (!open) break;
+        }
+      }
+    }
+    for (int q = 0; q < n; ++q)
+      if (inq[q]) b.qubits.push_back(q);
+    for (int& gi : b.gates) gi = order[gi];
+    blocks.push_back(std::move(b));
+  }
+  return blocks;
+}
+
+// ket's Fuser block rule on one barrier-free segment.
+std::vector<Block> reference_blocks(const ketgpu_op* ops, const std::vector<int>& order) {
+  std::vector<Block> blocks;
+  Block cur;
+  std::vector<int> first_qubits;
+  for (int idx : order) {
+    const ketgpu_op& o = ops[idx];
+    const int a = gate_arity(o.type);
+    bool subset = !cur.gates.empty();
+    for (int j = 0; j < a && subset; ++j)
+      if (std::find(first_qubits.begin(), first_qubits.end(), o.q[j]) == first_qubits.end()) subset = false;
+    if (!cur.gates.empty() && !subset) {
+      blocks.push_back(std::move(cur));
+      cur = Block();
+    }
+    if (cur.gates.empty()) {
+      first_qubits.assign(o.q, o.q + a);
+      cur.qubits = first_qubits;
+    }
+    cur.gates.push_back(idx);
+  }
+  if (!cur.gates.empty()) blocks.push_back(std::move(cur));
+  return blocks;
+}
+
+void emit_single(Plan& plan, const ketgpu_op& o, int idx) {
+  Pass p = lower_gate(o);
+  p.first_op = idx;
+  p.n_gates = 1;
+  plan.passes.push_back(p);
+}
+
+void emit_fused(Plan& plan, int n, const ketgpu_op* ops, const Block& b, const PlanOptions& opt) {
+  std::vector<const ketgpu_op*> gs;
+  for (int gi : b.gates) gs.push_back(&ops[gi]);
+  std::vector<int> qs = b.qubits;
+  std::sort(qs.begin(), qs.end());
+  const int k = (int)qs.size();
+  std::vector<cplx> mat = block_matrix(gs, qs.data(), k);
+  Pass p;
+  p.first_op = b.gates.front();
+  p.n_gates = (int)b.gates.size();
+  if (k == 1) {  // one 2x2 through the streaming pair kernel
+    p.kind = PassKind::Pair;
+    p.mode = kPairGeneral;
+    p.nfixed = 1;
+    p.fixed[0] = qs[0];
+    p.p0 = 0;
+    p.p1 = uint64_t{1} << qs[0];
+    for (int j = 0; j < 4; ++j) p.m[j] = mat[j];
+    plan.passes.push_back(p);
+    return;
+  }
+  p.kind = PassKind::Fused;
+  p.k = k;
+  for (int j = 0; j < k; ++j) p.qubits[j] = qs[j];
+  p.tensor = opt.precision == KETGPU_C64 && opt.tensor && tc_supported(k) && n >= k + 7;
+  p.mat_index = plan.matrices.size();
+  plan.matrices.push_back(std::move(mat));
+  plan.passes.push_back(p);
+}
+
+}  // namespace
+
+void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const PlanOptions& opt) {
+  plan.n = n;
+  plan.precision = opt.precision;
+  plan.passes.clear();
+  plan.matrices.clear();
+  uint64_t n_gates = 0;
+  double predicted = 0;
+  const size_t amp = opt.precision == KETGPU_C64 ? 8 : 16;
+  // Split at structural ops: they are fusion barriers (simulator.cpp:496).
+  std::vector<int> seg;
+  auto flush = [&]() {
+    if (seg.empty()) return;
+    if (opt.fusion == KETGPU_FUSE_NONE) {
+      for (int idx : seg) emit_single(plan, ops[idx], idx);
+    } else if (opt.fusion == KETGPU_FUSE_REFERENCE) {
+      for (const Block& b : reference_blocks(ops, seg)) {
+        if (b.gates.size() == 1) emit_single(plan, ops[b.gates[0]], b.gates[0]);
+        else emit_fused(plan, n, ops, b, opt);
+      }
+    } else {
+      const bool learned = opt.fusion == KETGPU_FUSE_LEARNED && learned_model_attached();
+      for (const Block& b : grow_blocks(n, ops, seg, std::max(1, opt.max_k))) {
+        if (b.gates.size() == 1) {
+          emit_single(plan, ops[b.gates[0]], b.gates[0]);
+          continue;
+        }
+        const int k = (int)b.qubits.size();
+        double separate = 0;
+        for (int gi : b.gates) separate += gate_traffic_fraction(ops[gi]);
+        bool fuse;
+        if (learned) {
+          std::vector<const ketgpu_op*> gs;
+          for (int gi : b.gates) gs.push_back(&ops[gi]);
+          std::vector<int> qs = b.qubits;
+          const float fused_us = learned_block_cost(n, gs, qs.data(), k);
+          double sep_us = 0;
+          for (int gi : b.gates) {
+            std::vector<const ketgpu_op*> one{&ops[gi]};
+            std::vector<int> q1;
+            for (int j = 0; j < gate_arity(ops[gi].type); ++j) q1.push_back(ops[gi].q[j]);
+            std::sort(q1.begin(), q1.end());
+            sep_us += learned_block_cost(n, one, q1.data(), (int)q1.size());
+          }
+          fuse = fused_us < sep_us;
+          predicted += fuse ? fused_us : sep_us;
+        } else {
+          fuse = fused_cost_static(k, opt.precision, opt.tensor) < separate;
+        }
+        if (fuse) {
+          emit_fused(plan, n, ops, b, opt);
+        } else {
+          for (int gi : b.gates) emit_single(plan, ops[gi], gi);
+        }
+      }
+    }
+    seg.clear();
+  };
+  for (uint64_t i = 0; i < nops; ++i) {
+    if (is_unitary(ops[i].type)) {
+      seg.push_back((int)i);
+      ++n_gates;
+    } else {
+      flush();
+    }
+  }
+  flush();
+  ketgpu_plan_stats& st = plan.stats;
+  st = ketgpu_plan_stats{};
+  st.n_gates = n_gates;
+  st.n_passes = plan.passes.size();
+  for (const Pass& p : plan.passes) {
+    st.bytes += p.bytes(n, amp);
+    if (p.kind == PassKind::Fused) {
+      ++st.n_fused;
+      if (p.tensor) ++st.n_tensor;
+      st.flops += 8.0 * (double)(1 << p.k) * (double)(uint64_t{1} << n);
+    }
+  }
+  st.predicted_us = predicted;
+}
+
+}  // namespace kb

@@ -1,0 +1,213 @@
+"""Parity of the CUDA path with the oracle and ket's golden outputs.
+
+Tolerances (written here, used throughout):
+  * complex128 mode: 1e-12 max-abs per amplitude (ket's own kTol,
+    tests/test_simulator.cpp:9);
+  * complex64 mode: 1e-5 max-abs per amplitude and fidelity > 1 - 1e-6.
+"""
+import ctypes as ct
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+FID32 = 1e-6
+
+MODES_128 = [("none", 5), ("reference", 5), ("greedy", 2), ("greedy", 3), ("greedy", 4), ("greedy", 5),
+             ("greedy", 6)]
+MODES_64 = [("none", 5, True), ("reference", 5, True), ("greedy", 3, True), ("greedy", 4, True),
+            ("greedy", 5, True), ("greedy", 5, False), ("greedy", 6, True)]
+
+
+def gpu_run(n, ops, precision="c128", fusion="greedy", k=5, tc=True):
+    import ket_b200 as kb
+    from ket_b200 import _lib
+    out = np.zeros(1 << n, dtype=np.complex128)
+    opt = kb.make_options(precision, fusion, k, tc)
+    _lib.check(_lib.lib.ketgpu_run(n, ops.ctypes.data, len(ops), ct.byref(opt), out.ctypes.data))
+    return out
+
+
+def fidelity(a, b):
+    return abs(np.vdot(a, b)) ** 2 / (np.vdot(a, a).real * np.vdot(b, b).real)
+
+
+def test_gate_battery_c128(golden):
+    g = golden("gate_battery")
+    for name, ops, want in zip(g["names"], g["ops"], g["states"]):
+        for fusion, k in MODES_128:
+            got = gpu_run(4, ops, "c128", fusion, k)
+            assert np.abs(got - want).max() < TOL64, (name, fusion, k)
+
+
+def test_gate_battery_c64(golden):
+    g = golden("gate_battery")
+    for name, ops, want in zip(g["names"], g["ops"], g["states"]):
+        got = gpu_run(4, ops, "c64", "none")
+        assert np.abs(got - want).max() < TOL32, name
+
+
+@pytest.mark.parametrize("n", [6, 10, 12])
+def test_random_mixed_c128_all_modes(golden, n):
+    g = golden("random_mixed")
+    want = g[f"state_{n}"]
+    for fusion, k in MODES_128:
+        got = gpu_run(n, g[f"ops_{n}"], "c128", fusion, k)
+        assert np.abs(got - want).max() < TOL64, (fusion, k)
+
+
+@pytest.mark.parametrize("n", [6, 10, 12])
+def test_random_mixed_c64_all_modes(golden, n):
+    g = golden("random_mixed")
+    want = g[f"state_{n}"]
+    for fusion, k, tc in MODES_64:
+        got = gpu_run(n, g[f"ops_{n}"], "c64", fusion, k, tc)
+        assert np.abs(got - want).max() < TOL32, (fusion, k, tc)
+        assert fidelity(got, want) > 1 - FID32, (fusion, k, tc)
+
+
+def _block_circuit(n, qubits, seed, depth=30):
+    """A dense random block on `qubits` (one fused pass when k = len(qubits))."""
+    from oracle.oracle import make_ops
+    rng = np.random.default_rng(seed)
+    gs = []
+    for q in qubits:
+        gs.append(("U", [q], rng.uniform(0, 2 * math.pi, 3).tolist()))
+    for _ in range(depth):
+        a, b = rng.choice(qubits, 2, replace=False).tolist()
+        gs.append(("CX", [a, b]))
+        gs.append(("U", [b], rng.uniform(0, 2 * math.pi, 3).tolist()))
+        gs.append(("CP", [a, b], [float(rng.uniform(0, 6.28))]))
+    return make_ops(gs)
+
+
+TARGETS = {
+    "low5": [0, 1, 2, 3, 4], "high5": None, "mixed5": [0, 3, 7, 11, 13], "spread5": [1, 5, 8, 12, 15],
+    "low4": [0, 1, 2, 3], "mixed4": [2, 6, 9, 14], "high4": None,
+}
+
+
+@pytest.mark.parametrize("name", sorted(TARGETS))
+@pytest.mark.parametrize("n", [12, 16, 18])
+def test_tensor_core_block_positions(oracle, name, n):
+    """Single dense blocks on the tcgen05 path at every kind of target set."""
+    import ket_b200 as kb
+    k = 5 if name.endswith("5") else 4
+    qs = TARGETS[name] or list(range(n - k, n))
+    qs = [q for q in qs if q < n]
+    if len(qs) != k:
+        pytest.skip("targets outside the register")
+    prep = _block_circuit(n, list(range(n)), seed=n, depth=2 * n)  # generic input state
+    blk = _block_circuit(n, qs, seed=100 + n)
+    ops = np.concatenate([prep, blk])
+    want = oracle.run(n, ops, fuse=0)
+    st = kb.plan_stats(kb.Circuit(n), None)  # warm import
+    got = gpu_run(n, ops, "c64", "greedy", k, True)
+    assert np.abs(got - want).max() < TOL32
+    assert fidelity(got, want) > 1 - FID32
+    # the block itself ran on the tensor cores
+    from ket_b200 import _lib
+    opt = kb.make_options("c64", "greedy", k, True)
+    h = ct.c_void_p()
+    _lib.check(_lib.lib.ketgpu_plan_create(n, blk.ctypes.data, len(blk), ct.byref(opt), ct.byref(h)))
+    s = _lib.PlanStats()
+    _lib.check(_lib.lib.ketgpu_plan_stats_get(h, ct.byref(s)))
+    _lib.lib.ketgpu_plan_destroy(h)
+    assert s.n_tensor >= 1
+
+
+def test_brickwork_20q_d20_c128(oracle, golden):
+    g = golden("brickwork_20q_d20")
+    ops = g["ops"]
+    want_full = oracle.run(20, ops, fuse=1)
+    assert np.array_equal(want_full[:4096], g["head"])
+    for fusion, k in [("none", 5), ("reference", 5), ("greedy", 5)]:
+        got = gpu_run(20, ops, "c128", fusion, k)
+        assert np.abs(got - want_full).max() < TOL64, fusion
+
+
+def test_brickwork_20q_d20_c64(oracle, golden):
+    g = golden("brickwork_20q_d20")
+    ops = g["ops"]
+    want = oracle.run(20, ops, fuse=1)
+    for fusion, k, tc in [("none", 5, True), ("greedy", 5, True), ("greedy", 4, True), ("greedy", 5, False)]:
+        got = gpu_run(20, ops, "c64", fusion, k, tc)
+        assert np.abs(got - want).max() < TOL32, fusion
+        assert fidelity(got, want) > 1 - FID32, fusion
+
+
+def test_expval_matches_golden(golden):
+    import ket_b200 as kb
+    g = golden("expval")
+    s = golden("random_mixed")["state_10"]
+    for prec, tol in (("c128", 1e-12), ("c64", 1e-6)):
+        d = kb.DeviceState(10, prec).from_numpy(s)
+        for p, v in zip(g["paulis"], g["values"]):
+            assert abs(d.expval(str(p)) - v) < tol, (prec, p)
+        terms = list(zip(g["coeffs"].tolist(), [str(p) for p in g["paulis"]]))
+        assert abs(d.expval(terms) - g["total"][0]) < 40 * tol
+        d.close()
+
+
+def test_expval_errors_like_ket():
+    import ket_b200 as kb
+    d = kb.DeviceState(2, "c128")
+    with pytest.raises(ValueError):
+        d.expval("Z")
+    with pytest.raises(ValueError):
+        d.expval("ZQ")
+    assert abs(d.expval("ZZ") - 1.0) < 1e-15
+    assert abs(d.expval("zi") - 1.0) < 1e-15
+
+
+def test_norm_and_inner():
+    import ket_b200 as kb
+    from ket_b200.workloads import random_brickwork
+    c = random_brickwork(16, 6, seed=3)
+    a = kb.run_device(c, "c128")
+    b = kb.run_device(c, "c128")
+    assert abs(a.norm() - 1) < 1e-12
+    assert abs(a.inner(b) - 1) < 1e-12
+
+
+def test_sampler_bit_exact_against_oracle(oracle, golden):
+    import ket_b200 as kb
+    s10 = golden("random_mixed")["state_10"]
+    m = golden("measure")
+    for prec in ("c128", "c64"):
+        d = kb.DeviceState(10, prec).from_numpy(s10)
+        host = d.to_numpy()
+        for seed in (42, 7, 2024):
+            u = m[f"uniforms_{seed}"]
+            got = d.sample(u)
+            want = oracle.sample_tree(10, host if prec == "c128" else host.astype(np.complex64), u)
+            assert np.array_equal(got, want), (prec, seed)
+            if prec == "c128":
+                assert np.array_equal(got, m[f"outcomes_{seed}"])  # = ket::measure on this stream
+        d.close()
+
+
+@pytest.mark.parametrize("n", [5, 6, 11, 16, 20])
+def test_sampler_tree_levels(oracle, n):
+    import ket_b200 as kb
+    from ket_b200.workloads import random_brickwork
+    c = random_brickwork(n, 4, seed=n)
+    d = kb.run_device(c, "c64")
+    host = d.to_numpy().astype(np.complex64)
+    u = kb.uniforms(99 + n, 20000)
+    u = np.concatenate([u, [0.0, np.nextafter(1.0, 0.0), 0.5]])
+    assert np.array_equal(d.sample(u), oracle.sample_tree(n, host, u))
+
+
+def test_uniform_stream_is_std_mt19937(golden):
+    import ket_b200 as kb
+    from ket_b200.workloads import MT19937
+    m = golden("measure")
+    for seed in (42, 7, 2024):
+        assert np.array_equal(kb.uniforms(seed, 2000), m[f"uniforms_{seed}"])
+    r = MT19937(42)
+    assert [r.canonical() for _ in range(5)] == list(m["uniforms_42"][:5])

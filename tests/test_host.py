@@ -1,0 +1,128 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports
+every symbol of include/ket_b200.h, the circuit recorder mirrors ket's
+validation, the uniform streams agree, and the planner (host code) builds
+the expected plans."""
+import ctypes as ct
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "ket_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(ketgpu_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    from ket_b200 import _lib
+    names = header_functions()
+    assert len(names) >= 30
+    for name in names:
+        assert hasattr(_lib.lib, name), name
+    assert _lib.lib.ketgpu_abi_version() == 1
+
+
+def test_circuit_validation_mirrors_ket():
+    import ket_b200 as ket
+    c = ket.Circuit(3)
+    with pytest.raises(IndexError):
+        c.x(3)
+    with pytest.raises(ValueError):
+        c.ccx(0, 1, 0)
+    with pytest.raises(ValueError):
+        c.append(ket.Circuit(2), [0])
+    c.measure(2, 5)
+    assert c.n_clbits == 6
+    c.probe()
+    c.probe("x")
+    assert [g.label for g in c.gates if g.type == ket.GateType.Probe] == ["ψ0", "x"]
+
+
+def test_op_layout_and_codes():
+    import ket_b200 as ket
+    from ket_b200._lib import OP_DTYPE
+    assert OP_DTYPE.itemsize == 48
+    c = ket.Circuit(3)
+    c.cu(2, 0, 0.1, 0.2, 0.3)
+    c.measure(1, 4)
+    ops = c.to_ops()
+    assert ops[0]["type"] == 19 and list(ops[0]["q"][:2]) == [2, 0]
+    assert list(ops[0]["p"]) == [0.1, 0.2, 0.3]
+    assert ops[1]["type"] == 24 and ops[1]["q"][1] == 4
+
+
+def test_clifford_detection():
+    import ket_b200 as ket
+    c = ket.Circuit(2)
+    for g in ("h", "x", "y", "z", "s", "sdg"):
+        getattr(c, g)(0)
+    c.cx(0, 1)
+    c.cy(1, 0)
+    c.cz(0, 1)
+    c.swap(0, 1)
+    c.barrier()
+    c.measure_all()
+    assert ket.is_clifford(c) and ket.chosen_method(c) == "stabilizer"
+    sub = ket.Circuit(1)
+    sub.t(0)
+    c.append(sub, [1])
+    assert not ket.is_clifford(c)
+
+
+def test_uniform_streams_agree(oracle):
+    import ket_b200 as ket
+    from ket_b200.workloads import MT19937
+    for seed in (0, 1, 42, 2**32 - 1):
+        a = ket.uniforms(seed, 1500)
+        assert np.array_equal(a, oracle.uniforms(seed, 1500))
+        r = MT19937(seed)
+        assert [r.canonical() for _ in range(3)] == list(a[:3])
+
+
+def test_plans_on_the_host():
+    import ket_b200 as ket
+    from ket_b200.workloads import random_brickwork
+    c = random_brickwork(30, 40)
+    un = ket.plan_stats(c, ket.make_options("c64", "none"))
+    gr = ket.plan_stats(c, ket.make_options("c64", "greedy", 5, True))
+    assert un["n_passes"] == 1780 and un["n_gates"] == 1780
+    assert gr["n_passes"] < un["n_passes"] / 8
+    assert gr["n_tensor"] == gr["n_fused"] > 0
+    # algorithmic bytes: 1200 dense 1q passes + 580 CX passes over half the state
+    assert un["bytes"] == 1200 * 16 * 2**30 + 580 * 8 * 2**30
+    assert gr["bytes"] < un["bytes"] / 8
+
+
+def test_plan_errors():
+    import ket_b200 as ket
+    from ket_b200 import _lib
+    ops = np.zeros(1, dtype=_lib.OP_DTYPE)
+    ops[0]["type"] = 13
+    ops[0]["q"][:2] = [0, 5]
+    h = ct.c_void_p()
+    opt = ket.make_options("c64")
+    rc = _lib.lib.ketgpu_plan_create(3, ops.ctypes.data, 1, ct.byref(opt), ct.byref(h))
+    assert rc == _lib.ERR_OUT_OF_RANGE
+    assert "out of range" in _lib.lib.ketgpu_last_error().decode()
+    ops[0]["q"][:2] = [1, 1]
+    rc = _lib.lib.ketgpu_plan_create(3, ops.ctypes.data, 1, ct.byref(opt), ct.byref(h))
+    assert rc == _lib.ERR_INVALID
+    bad = ket.make_options("c64", "greedy", 9)
+    ops[0]["q"][:2] = [0, 1]
+    assert _lib.lib.ketgpu_plan_create(3, ops.ctypes.data, 1, ct.byref(bad), ct.byref(h)) == _lib.ERR_INVALID
+
+
+def test_workload_shapes():
+    from ket_b200.workloads import qft_ghz_rz, random_mixed, variational_ansatz
+    c = qft_ghz_rz(33)
+    assert len(c.gates) == 33 + 528 + 1 + 32 + 33
+    a, pidx = variational_ansatz(24, 8)
+    assert (pidx >= 0).sum() == 384 and len(a.gates) == 8 * 72
+    m = random_mixed(22, 20, seed=3)
+    used = sum(len(g.qubits) for g in m.gates)
+    assert used == 22 * 20
