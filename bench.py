@@ -182,8 +182,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-checks", action="store_true")
     ap.add_argument("--fusion", default="greedy")
     ap.add_argument("--k", type=int, default=5)
+    ap.add_argument("--qubits", type=int, default=N_QUBITS, help="smaller cases for profiling only")
+    ap.add_argument("--depth", type=int, default=DEPTH)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -194,10 +197,11 @@ def main():
     from ket_b200.workloads import random_brickwork
     lib = _lib.lib
 
-    circ = random_brickwork(N_QUBITS, DEPTH, SEED)
+    nq = args.qubits
+    circ = random_brickwork(nq, args.depth, SEED)
     ops = circ.to_ops()
     opt = ket.make_options("c64", args.fusion, args.k, True)
-    plan = ket.Plan(N_QUBITS, ops, opt)
+    plan = ket.Plan(nq, ops, opt)
     stats = plan.stats()
     npass = int(stats["n_passes"])
     info = []
@@ -205,7 +209,7 @@ def main():
         kind, k, tc, b = ct.c_int32(), ct.c_int32(), ct.c_int32(), ct.c_double()
         _lib.check(lib.ketgpu_plan_pass_info(plan._h, i, ct.byref(kind), ct.byref(k), ct.byref(tc), ct.byref(b)))
         info.append((kind.value, k.value, tc.value, b.value))
-    state = ket.DeviceState(N_QUBITS, "c64")
+    state = ket.DeviceState(nq, "c64")
     import torch
     stream = torch.cuda.ExternalStream(lib.ketgpu_state_stream(state.handle))
     pass_ms = np.zeros(npass, dtype=np.float32)
@@ -246,8 +250,33 @@ def main():
     ms_step = ms_total / args.steps
     value = ms_step / world  # aggregate: N circuits per step over N replicas
 
-    # correctness guard on the timed state: unit norm
-    nrm = state.norm()
+    # accuracy of the timed state against the complex128 path (FP64 SIMT
+    # blocks, itself pinned to ket's complex128 ket::run at 1e-12 by the
+    # tests), and the plain per-gate GPU method for the fusion speed-up
+    checks = {"norm": state.norm()}
+    if not args.no_checks:
+        ref = ket.DeviceState(nq, "c128")
+        ref_plan = ket.Plan(nq, ops, ket.make_options("c128", "greedy", 5, True))
+        ref_plan.execute(ref)
+        cmp = state.compare(ref)
+        checks.update({"max_abs_vs_c128": cmp["max_abs"], "fidelity_vs_c128": cmp["fidelity"],
+                       "fidelity_unnormalised_vs_c128": cmp["fidelity_unnormalised"]})
+        ref.close()
+        ref_plan.close()
+        un_plan = ket.Plan(nq, ops, ket.make_options("c64", "none"))
+        un_ms = []
+        for _ in range(2):
+            _lib.check(lib.ketgpu_state_reset(state.handle))
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            _lib.check(lib.ketgpu_plan_execute(un_plan._h, state.handle))
+            a1.record(stream)
+            _lib.check(lib.ketgpu_state_synchronize(state.handle))
+            un_ms.append(a0.elapsed_time(a1))
+        checks["unfused_ms"] = min(un_ms)
+        checks["speedup_vs_unfused"] = min(un_ms) / ms_step
+        un_plan.close()
 
     # dense-block kernel roofline (tensor-core passes)
     tc_idx = [i for i, x in enumerate(info) if x[0] == 2 and x[2] == 1]
@@ -270,13 +299,13 @@ def main():
     # e2e through the C ABI with host buffers
     e2e = None
     if args.e2e_steps > 0:
-        out = np.empty(1 << N_QUBITS, dtype=np.complex128)
+        out = np.empty(1 << nq, dtype=np.complex128)
         ops_pinned = ops.copy()
         ts = []
         for i in range(args.e2e_steps + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            _lib.check(lib.ketgpu_run(N_QUBITS, ops_pinned.ctypes.data, len(ops_pinned), ct.byref(opt),
+            _lib.check(lib.ketgpu_run(nq, ops_pinned.ctypes.data, len(ops_pinned), ct.byref(opt),
                                       out.ctypes.data))
             t1 = time.perf_counter()
             if i > 0:
@@ -284,12 +313,12 @@ def main():
         e2e_ms = barrier_max(statistics.median(ts), world) / world
         mat_bytes = int(stats["n_tensor"]) * 2 * 64 * 64 * 4
         e2e = {"value": e2e_ms, "unit": "ms/circuit", "h2d_bytes_per_step": int(ops.nbytes) + mat_bytes,
-               "d2h_bytes_per_step": (1 << N_QUBITS) * 8,
+               "d2h_bytes_per_step": (1 << nq) * 8,
                "note": "ketgpu_run: host ops in, 2^30 amplitudes out to a host complex128 buffer"}
         del out
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and nq == N_QUBITS and args.depth == DEPTH:
         try:
             cpu = cpu_baseline_reference(ops)
         except Exception as ex:  # the reference build may be absent
@@ -307,7 +336,7 @@ def main():
                        "l2": "state 8 GiB > L2 126 MB, no flush", "gates": int(stats["n_gates"]),
                        "passes": npass, "tensor_passes": int(stats["n_tensor"])},
             "roofline": roof, "passes": pass_summary, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(launches), "clocks": clocks, "norm": nrm,
+            "gpu_launches": int(launches), "clocks": clocks, "checks": checks,
         }
         print(json.dumps(line), flush=True)
     state.close()

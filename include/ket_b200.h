@@ -146,6 +146,9 @@ int ketgpu_run(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
 int ketgpu_norm(const ketgpu_state* s, double* out);
 /* <a|b> (complex) -- fidelity checks. */
 int ketgpu_inner(const ketgpu_state* a, const ketgpu_state* b, double* re, double* im);
+/* Compare two states of any precisions: out5 = {max |a_i - b_i| over re and
+ * im parts, Re <a|b>, Im <a|b>, <a|a>, <b|b>} (FP64 sums). */
+int ketgpu_compare(const ketgpu_state* a, const ketgpu_state* b, double* out5);
 /* Replaces ket::expval(State, string) (include/ket/observable.hpp:24,
  * src/observable.cpp:18-83): same masks, same right-to-left order, same
  * errors (length / character -> KETGPU_ERR_INVALID). */

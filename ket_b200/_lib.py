@@ -80,6 +80,7 @@ def _load():
         "ketgpu_run": ([i32, vp, u64, ct.POINTER(Options), vp], ct.c_int),
         "ketgpu_norm": ([vp, pd], ct.c_int),
         "ketgpu_inner": ([vp, vp, pd, pd], ct.c_int),
+        "ketgpu_compare": ([vp, vp, vp], ct.c_int),
         "ketgpu_expval": ([vp, ct.c_char_p, pd], ct.c_int),
         "ketgpu_expval_sum": ([vp, vp, vp, u64, pd], ct.c_int),
         "ketgpu_expval_terms": ([vp, vp, u64, vp], ct.c_int),

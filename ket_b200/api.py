@@ -132,6 +132,15 @@ class DeviceState:
         check(lib.ketgpu_inner(self._h, other._h, ct.byref(re), ct.byref(im)))
         return complex(re.value, im.value)
 
+    def compare(self, other: "DeviceState") -> dict:
+        """max |a-b|, fidelity |<a|b>|^2/(<a|a><b|b>), overlap and norms (any precisions)."""
+        out = np.zeros(5)
+        check(lib.ketgpu_compare(self._h, other._h, out.ctypes.data))
+        ov = complex(out[1], out[2])
+        return {"max_abs": float(out[0]), "overlap": ov, "norm_a": float(out[3]), "norm_b": float(out[4]),
+                "fidelity": abs(ov) ** 2 / (out[3] * out[4]) if out[3] > 0 and out[4] > 0 else 0.0,
+                "fidelity_unnormalised": abs(ov) ** 2}
+
     def expval(self, obs) -> float:
         return _expval_dev(self, obs)
 

@@ -586,3 +586,12 @@ KB_API int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* 
 KB_API void* ketgpu_state_stream(const ketgpu_state* s) {
   return s ? reinterpret_cast<void*>(as_state(s)->stream) : nullptr;
 }
+
+KB_API int ketgpu_compare(const ketgpu_state* a, const ketgpu_state* b, double* out5) {
+  return guard([&] {
+    need(a && b && out5, "null argument");
+    need(as_state(a)->n == as_state(b)->n, "states differ in size");
+    DeviceGuard g(as_state(a)->device);
+    compare_states(*as_state(a), *as_state(b), out5);
+  });
+}

@@ -38,10 +38,10 @@ __device__ int g_tc_error = 0;
 
 namespace {
 
-constexpr int kTcThreads = 256;
+constexpr int kTcThreads = 416;
 constexpr int kGroupBits = 7;  // M = 128 rows
-constexpr int kSlots = 3;
 constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr int kSmemBudget = 232448 - 1024;  // opt-in limit less static shared memory
 
 template <int KQ>
 struct TcCfg {
@@ -50,19 +50,28 @@ struct TcCfg {
   static constexpr int N = 2 * DIM;           // accumulator columns
   static constexpr int TB = KQ + kGroupBits;  // tile bits
   static constexpr int TILE = 1 << TB;        // amplitudes per tile
-  static constexpr int RAW_BYTES = TILE * 8;
-  static constexpr int KBLK = (K * 4) / 128;      // 128-byte swizzle atoms along K
-  static constexpr int A_BYTES = 128 * K * 4;     // one A image (hi or lo)
-  static constexpr int B_BYTES = N * K * 4;       // one B image
-  static constexpr int KSTEPS = K / 8;            // tf32 MMA K = 8
-  static constexpr int TMEM_COLS = 2 * N;         // two accumulators
-  static constexpr size_t SMEM = (size_t)kSlots * RAW_BYTES + 2 * A_BYTES + 2 * B_BYTES + 1024;
+  static constexpr int RAW_BYTES = TILE * 8;  // one staging image (= one A image)
+  static constexpr int B_BYTES = N * K * 4;   // one B image
+  static constexpr int KSTEPS = K / 8;        // tf32 MMA K = 8
+  // tensor memory: per tile parity an A region (hi | lo, 2K columns) and an
+  // accumulator region (main | correction, 2N columns)
+  static constexpr int A_COLS = 2 * K;
+  static constexpr int ACC_COLS = 2 * N;
+  static constexpr int TMEM_COLS = 2 * A_COLS + 2 * ACC_COLS;
+  // staging images: as many as fit next to the B images (loads in flight)
+  static constexpr int SLOTS_FIT = (kSmemBudget - 1024 - 2 * B_BYTES) / RAW_BYTES;
+  static constexpr int SLOTS = SLOTS_FIT > 12 ? 12 : SLOTS_FIT;
+  static constexpr size_t SMEM = (size_t)SLOTS * RAW_BYTES + 2 * B_BYTES + 1024;  // + alignment slack
+  static_assert(TMEM_COLS <= 512, "tensor memory budget");
+  static_assert(SLOTS >= 3, "shared memory budget");
 };
 
 struct TcGeom {
-  int tb;
-  int tile_pos[16];
+  int tile_pos[16];   // tile qubits, ascending
   int is_target[16];
+  int m_low;          // tile qubits 0..m_low-1 form the low run
+  int nh;             // tile qubits above the low run
+  int hpos[16];
   uint64_t n_tiles;
 };
 
@@ -86,39 +95,15 @@ __host__ __device__ __forceinline__ uint32_t sw128_offset(int row, int kk, int r
   return (uint32_t)(kb * rows * 128 + row * 128 + ((chunk ^ (row & 7)) << 4) + ((kk & 3) << 2));
 }
 
-__device__ __forceinline__ float tf32_hi(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-
 __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+__device__ __forceinline__ void cp_async8(uint32_t saddr, const void* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr), "l"(g) : "memory");
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-// Bounded wait for the completion of the phase with the given parity.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t it = 0; it < kWaitLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
 }
 
 __device__ __forceinline__ void fence_proxy_async() {
@@ -131,13 +116,24 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-__device__ __forceinline__ void tc_mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                            uint32_t idesc, uint32_t accumulate) {
+// A from tensor memory (lanes = rows, columns = K), B from shared memory.
+__device__ __forceinline__ void tc_mma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
+                                               uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// 32 lanes x 16 columns of 32-bit values from the warp's registers.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
       : "memory");
 }
 
@@ -146,8 +142,11 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
                : "memory");
 }
 
-// 32 lanes x 16 columns (x16) of 32-bit accumulator per warp.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+// 32 lanes x NC columns of 32-bit accumulator per warp.
+template <int NC>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float* v);
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float* v) {
   uint32_t r[16];
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
@@ -168,59 +167,56 @@ __host__ __device__ constexpr uint32_t tf32_idesc() {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
+// Roles (13 warps): 0-3 producers (cp.async into staging images), 4-7
+// converters (hi/lo split into the A images), 8-11 epilogue (TMEM -> staging
+// -> HBM; warp w reads TMEM lanes 32*(w%4)..+31), 12 the MMA issuer.
+// mbarriers hand each tile from stage to stage, so loads of later tiles,
+// the split of tile j+1, the MMAs of tile j and the drain of tile j-1
+// proceed concurrently.
+constexpr int kProducers = 128, kConverters = 128, kEpilogue = 128;
+
 template <int KQ>
 __global__ void __launch_bounds__(kTcThreads, 1)
     fused_tc_kernel(float2* __restrict__ s, TcGeom g, const uint32_t* __restrict__ bimg) {
   using Cfg = TcCfg<KQ>;
-  constexpr int DIM = Cfg::DIM, N = Cfg::N, TILE = Cfg::TILE;
+  constexpr int N = Cfg::N, TILE = Cfg::TILE;
+  constexpr int CPT = TILE / 2 / kProducers;  // 16-byte chunks per producer / epilogue thread
+  constexpr int S = Cfg::SLOTS;
+  constexpr int K = Cfg::K;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
-  // 1024-byte align the operand region for the 128B swizzle atoms.
-  unsigned char* base_ptr =
-      smem_dyn + ((1024 - (smem_u32(smem_dyn) & 1023)) & 1023);
-  unsigned char* a_hi = base_ptr;
-  unsigned char* a_lo = a_hi + Cfg::A_BYTES;
-  unsigned char* b_hi = a_lo + Cfg::A_BYTES;
+  // [B hi][B lo][staging image 0..S-1]; a staging image receives the raw
+  // tile in the A layout, is read once by the converters (which put hi and lo
+  // into tensor memory), and then carries the accumulator back out.
+  unsigned char* base_ptr = smem_dyn + ((1024 - (smem_u32(smem_dyn) & 1023)) & 1023);
+  unsigned char* b_hi = base_ptr;
   unsigned char* b_lo = b_hi + Cfg::B_BYTES;
-  unsigned char* raw = b_lo + Cfg::B_BYTES;  // kSlots x RAW_BYTES
+  unsigned char* raw = b_lo + Cfg::B_BYTES;
 
-  __shared__ uint64_t off_lo[64], off_hi[64];
-  __shared__ int gc_lo[64], gc_hi[64];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t bar_full[S], bar_free[S];
+  __shared__ __align__(8) uint64_t bar_a_ready[2], bar_mma[2], bar_acc_free[2];
   __shared__ uint32_t tmem_base_slot;
+  __shared__ uint64_t base_ring[2 * S];
+  __shared__ volatile int abort_flag;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  // ---- lookup tables: address-order tile index e -> global offset / (g, c)
-  if (tid < 128) {
-    const int half = tid >> 6, e = tid & 63;
-    uint64_t off = 0;
-    int gc = 0, tcount = 0, gcount = 0;
-    for (int j = 0; j < g.tb; ++j) {
-      const bool t = g.is_target[j];
-      const int sh = t ? tcount++ : (KQ + gcount++);
-      const int local = j - 6 * half;
-      if (local >= 0 && local < 6 && ((e >> local) & 1)) {
-        off |= uint64_t{1} << g.tile_pos[j];
-        gc |= 1 << sh;
-      }
+  if (tid == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(smem_u32(&bar_full[i]), kProducers + 1);
+      mbar_init(smem_u32(&bar_free[i]), kEpilogue);
     }
-    if (half == 0) {
-      off_lo[e] = off;
-      gc_lo[e] = gc;
-    } else {
-      off_hi[e] = off;
-      gc_hi[e] = gc;
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(smem_u32(&bar_a_ready[i]), kConverters);
+      mbar_init(smem_u32(&bar_mma[i]), 1);
+      mbar_init(smem_u32(&bar_acc_free[i]), kEpilogue);
     }
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // ---- B images (hi, lo) into shared memory
   {
     const uint4* src = reinterpret_cast<const uint4*>(bimg);
     uint4* dst = reinterpret_cast<uint4*>(b_hi);
     for (int i = tid; i < (2 * Cfg::B_BYTES) / 16; i += kTcThreads) dst[i] = src[i];
-  }
-  if (tid == 0) {
-    mbar_init(smem_u32(&mbar), 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -238,132 +234,198 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint64_t first = blockIdx.x;
   const uint64_t stride = gridDim.x;
   const uint64_t count = first < g.n_tiles ? (g.n_tiles - first + stride - 1) / stride : 0;
+  const bool q0_group = !g.is_target[0];
 
+  // Bounded wait; on timeout raise the flags and let every role leave.
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+      uint32_t done;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(done)
+          : "r"(a), "r"(parity)
+          : "memory");
+      if (done) return true;
+      if ((it & 255) == 255 && abort_flag) return false;
+    }
+    abort_flag = 1;
+    atomicExch(&g_tc_error, 1);
+    return false;
+  };
+  auto arrive = [](uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+  };
+
+  // Chunk offsets shared by producers and epilogue threads: chunk
+  // ch = t + 128*i covers tile amplitudes e = 2ch, 2ch+1 (address order, bit j
+  // of e <-> qubit g.tile_pos[j]); goff = offset of e in the state from the
+  // tile base, soff = byte offset of e in an A-layout image (row = group with
+  // a group bit at qubit 0 rotated to row bit 6, kk = 2*comb).  Amplitude e+1
+  // sits at soff + 8 (qubit 0 is the lowest target: next combination) or at
+  // soff + 8192 (qubit 0 is a group bit: row + 64).
+  const uint32_t pair_step = q0_group ? 64u * 128u : 8u;
+  auto chunk_offsets = [&](int t, uint64_t* goff, uint32_t* soff) {
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) {
+      const int e = 2 * (t + kProducers * i);
+      uint64_t off = 0;
+      int grp = 0, comb = 0, gb = 0, cb = 0;
+      for (int j = 0; j < Cfg::TB; ++j) {
+        const int bit = (e >> j) & 1;
+        if (g.is_target[j]) comb |= bit << cb++;
+        else grp |= bit << gb++;
+        if (bit) off |= uint64_t{1} << g.tile_pos[j];
+      }
+      const int row = q0_group ? ((grp >> 1) | ((grp & 1) << (kGroupBits - 1))) : grp;
+      goff[i] = off;
+      soff[i] = sw128_offset(row, 2 * comb, 128);
+    }
+  };
   auto tile_base = [&](uint64_t t) -> uint64_t {
-    uint64_t b = t;
-    for (int j = 0; j < g.tb; ++j) {
-      const int f = g.tile_pos[j];
+    uint64_t b = t << g.m_low;
+    for (int j = 0; j < g.nh; ++j) {
+      const int f = g.hpos[j];
       b = ((b >> f) << (f + 1)) | (b & ((uint64_t{1} << f) - 1));
     }
     return b;
   };
-  auto issue_load = [&](uint64_t j) {
-    if (j < count) {
+
+  if (warp < 4) {
+    // ------------------------------------------------------------ producers
+    uint64_t goff[CPT];
+    uint32_t soff[CPT];
+    chunk_offsets(tid, goff, soff);
+    for (uint64_t j = 0; j < count; ++j) {
+      const int slot = (int)(j % S);
+      if (j >= (uint64_t)S && !wait(&bar_free[slot], (uint32_t)(((j / S) - 1) & 1))) break;
       const uint64_t base = tile_base(first + j * stride);
-      const uint32_t slot = smem_u32(raw + (j % kSlots) * Cfg::RAW_BYTES);
-      for (int ch = tid; ch < TILE / 2; ch += kTcThreads) {
-        const int e = 2 * ch;
-        const uint64_t off = off_lo[e & 63] + off_hi[e >> 6];
-        cp_async16(slot + (uint32_t)e * 8u, s + base + off);
-      }
-    }
-    cp_async_commit();
-  };
-  // Drain one accumulator through shared memory (slot `out`, [g][c ^ (g mod DIM)]).
-  auto epilogue = [&](uint64_t j, unsigned char* out) {
-    const int q = warp & 3, h = warp >> 2;
-    const int row = 32 * q + lane;
-    float2* o2 = reinterpret_cast<float2*>(out);
-    const uint32_t acc = tmem + (uint32_t)((j & 1) * N);
+      const uint32_t dst = smem_u32(raw + slot * Cfg::RAW_BYTES);
+      const float2* src = s + base;
 #pragma unroll
-    for (int part = 0; part < N / 2 / 16; ++part) {
-      float v[16];
-      tmem_ld16(acc + ((uint32_t)(32 * q) << 16) + (uint32_t)(h * (N / 2) + part * 16), v);
-      tmem_ld_wait();
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int c = h * (DIM / 2) + part * 8 + i;
-        o2[row * DIM + (c ^ (row & (DIM - 1)))] = make_float2(v[2 * i], v[2 * i + 1]);
-      }
-    }
-    tc_fence_before();
-    __syncthreads();
-    const uint64_t base = tile_base(first + j * stride);
-    for (int ch = tid; ch < TILE / 2; ch += kTcThreads) {
-      const int e = 2 * ch;
-      const int gc0 = gc_lo[e & 63] + gc_hi[e >> 6];
-      const int gc1 = gc_lo[(e + 1) & 63] + gc_hi[(e + 1) >> 6];
-      const int g0 = gc0 >> KQ, c0 = gc0 & (DIM - 1);
-      const int g1 = gc1 >> KQ, c1 = gc1 & (DIM - 1);
-      const float2 x = o2[g0 * DIM + (c0 ^ (g0 & (DIM - 1)))];
-      const float2 y = o2[g1 * DIM + (c1 ^ (g1 & (DIM - 1)))];
-      const uint64_t off = off_lo[e & 63] + off_hi[e >> 6];
-      *reinterpret_cast<float4*>(s + base + off) = make_float4(x.x, x.y, y.x, y.y);
-    }
-    __syncthreads();
-  };
-
-  constexpr uint32_t idesc = tf32_idesc<N>();
-  bool ok = true;
-
-  issue_load(0);
-  issue_load(1);
-  issue_load(2);
-  for (uint64_t j = 0; j < count && ok; ++j) {
-    cp_async_wait<2>();
-    __syncthreads();
-    if (j >= 1) {
-      const bool done = mbar_wait(smem_u32(&mbar), (uint32_t)((j - 1) & 1));
-      if (__syncthreads_or(!done)) {  // the CTA leaves together
-        ok = false;
-        if (tid == 0) atomicExch(&g_tc_error, 1);
-        break;
-      }
-      tc_fence_after();
-    }
-    // ---- split raw tile j into the swizzled hi/lo A images
-    {
-      const float4* r4 = reinterpret_cast<const float4*>(raw + (j % kSlots) * Cfg::RAW_BYTES);
-      for (int ch = tid; ch < TILE / 2; ch += kTcThreads) {
-        const float4 v = r4[ch];
-        const int e = 2 * ch;
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int gc = gc_lo[(e + u) & 63] + gc_hi[(e + u) >> 6];
-          const int row = gc >> KQ, c = gc & (DIM - 1);
-          const float re = u ? v.z : v.x, im = u ? v.w : v.y;
-          const float hr = tf32_hi(re), hi_ = tf32_hi(im);
-          const uint32_t off = sw128_offset(row, 2 * c, 128);
-          *reinterpret_cast<float2*>(a_hi + off) = make_float2(hr, hi_);
-          *reinterpret_cast<float2*>(a_lo + off) = make_float2(re - hr, im - hi_);
+      for (int i = 0; i < CPT; ++i) {
+        if (q0_group) {
+          cp_async8(dst + soff[i], src + goff[i]);
+          cp_async8(dst + soff[i] + pair_step, src + goff[i] + 1);
+        } else {
+          cp_async16(dst + soff[i], src + goff[i]);
         }
       }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&bar_full[slot]))
+                   : "memory");
+      if (tid == 0) {
+        base_ring[j % (2 * S)] = base;
+        arrive(&bar_full[slot]);
+      }
     }
-    fence_proxy_async();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (tid == 0) {
-      const uint32_t acc = tmem + (uint32_t)((j & 1) * N);
-      const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
-      const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp < 8) {
+    // ----------------------------------------------------------- converters
+    // Thread = A row (TMEM lane 32*(warp%4) + lane): read the row from the
+    // staging image, split x = hi + lo with hi = tf32(x) (round to nearest,
+    // ties away: magnitude bits plus half an ulp, truncated) and
+    // lo = tf32(x - hi), and store both into the A region of tile parity j%2
+    // in tensor memory once the MMAs of tile j-2 have released it.
+    const int q = warp & 3;
+    const int row = 32 * q + lane;
+    const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+    for (uint64_t j = 0; j < count; ++j) {
+      const int slot = (int)(j % S);
+      if (!wait(&bar_full[slot], (uint32_t)((j / S) & 1))) break;
+      if (j >= 2 && !wait(&bar_mma[j & 1], (uint32_t)(((j - 2) >> 1) & 1))) break;
+      tc_fence_after();
+      const unsigned char* img = raw + slot * Cfg::RAW_BYTES;
+      const uint32_t areg = tmem + lane_off + (uint32_t)((j & 1) * Cfg::A_COLS);
+#pragma unroll
+      for (int part = 0; part < K / 16; ++part) {
+        uint32_t hi[16], lo[16];
+#pragma unroll
+        for (int c4 = 0; c4 < 4; ++c4) {
+          const uint4 x = *reinterpret_cast<const uint4*>(img + sw128_offset(row, part * 16 + 4 * c4, 128));
+          const uint32_t xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint32_t h = (xs[u] + 0x1000u) & 0xffffe000u;
+            hi[4 * c4 + u] = h;
+            lo[4 * c4 + u] = (__float_as_uint(__uint_as_float(xs[u]) - __uint_as_float(h)) + 0x1000u) & 0xffffe000u;
+          }
+        }
+        tmem_st16(areg + (uint32_t)(part * 16), hi);
+        tmem_st16(areg + (uint32_t)(K + part * 16), lo);
+      }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      tc_fence_before();
+      arrive(&bar_a_ready[j & 1]);
+    }
+  } else if (warp < 12) {
+    // ------------------------------------------------------------- epilogue
+    const int t = tid - 256;
+    const int q = warp & 3;
+    const int row = 32 * q + lane;
+    uint64_t goff[CPT];
+    uint32_t soff[CPT];
+    chunk_offsets(t, goff, soff);
+    for (uint64_t j = 0; j < count; ++j) {
+      const int slot = (int)(j % S);
+      if (!wait(&bar_mma[j & 1], (uint32_t)((j >> 1) & 1))) break;
+      tc_fence_after();
+      unsigned char* out = raw + slot * Cfg::RAW_BYTES;
+      const uint32_t acc = tmem + (uint32_t)(2 * Cfg::A_COLS + (j & 1) * Cfg::ACC_COLS) + ((uint32_t)(32 * q) << 16);
+#pragma unroll
+      for (int part = 0; part < N / 16; ++part) {
+        float vm[16], vc[16];
+        tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
+        tmem_ld<16>(acc + (uint32_t)(N + part * 16), vc);
+        tmem_ld_wait();
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          *reinterpret_cast<float4*>(out + sw128_offset(row, part * 16 + 4 * i, 128)) =
+              make_float4(vm[4 * i] + vc[4 * i], vm[4 * i + 1] + vc[4 * i + 1], vm[4 * i + 2] + vc[4 * i + 2],
+                          vm[4 * i + 3] + vc[4 * i + 3]);
+      }
+      tc_fence_before();
+      arrive(&bar_acc_free[j & 1]);
+      asm volatile("bar.sync 1, %0;" ::"n"(kEpilogue) : "memory");
+      float2* dst = s + base_ring[j % (2 * S)];
+#pragma unroll
+      for (int i = 0; i < CPT; ++i) {
+        float4 w;
+        if (q0_group) {
+          const float2 x = *reinterpret_cast<const float2*>(out + soff[i]);
+          const float2 y = *reinterpret_cast<const float2*>(out + soff[i] + pair_step);
+          w = make_float4(x.x, x.y, y.x, y.y);
+        } else {
+          w = *reinterpret_cast<const float4*>(out + soff[i]);
+        }
+        *reinterpret_cast<float4*>(dst + goff[i]) = w;
+      }
+      arrive(&bar_free[slot]);
+    }
+  } else if (warp == 12 && lane == 0) {
+    // ------------------------------------------------------------ MMA issue
+    constexpr uint32_t idesc = tf32_idesc<N>();
+    const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+    for (uint64_t j = 0; j < count; ++j) {
+      if (!wait(&bar_a_ready[j & 1], (uint32_t)((j >> 1) & 1))) break;
+      if (j >= 2 && !wait(&bar_acc_free[j & 1], (uint32_t)(((j >> 1) - 1) & 1))) break;
+      tc_fence_after();
+      const uint32_t acc = tmem + (uint32_t)(2 * Cfg::A_COLS + (j & 1) * Cfg::ACC_COLS);
+      const uint32_t ah = tmem + (uint32_t)((j & 1) * Cfg::A_COLS);
+      const uint32_t al = ah + (uint32_t)K;
 #pragma unroll
       for (int st = 0; st < Cfg::KSTEPS; ++st) {
-        const uint32_t ka = (uint32_t)((st >> 2) * 128 * 128 + (st & 3) * 32);
         const uint32_t kbo = (uint32_t)((st >> 2) * N * 128 + (st & 3) * 32);
-        tc_mma_tf32(acc, sw128_desc(ah + ka), sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
-        tc_mma_tf32(acc, sw128_desc(ah + ka), sw128_desc(bl + kbo), idesc, 1u);
-        tc_mma_tf32(acc, sw128_desc(al + ka), sw128_desc(bh + kbo), idesc, 1u);
+        // main term hi*hi in its own accumulator; the two correction terms
+        // (2^-11 smaller) in a second one, summed in FP32 by the epilogue
+        tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
+        tc_mma_tf32_ts(acc + N, ah + 8 * st, sw128_desc(bl + kbo), idesc, st > 0 ? 1u : 0u);
+        tc_mma_tf32_ts(acc + N, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
       }
-      tc_commit(smem_u32(&mbar));
-    }
-    if (j >= 1) epilogue(j - 1, raw + (j % kSlots) * Cfg::RAW_BYTES);
-    else __syncthreads();
-    issue_load(j + kSlots);
-  }
-  if (ok && count > 0) {
-    const bool done = mbar_wait(smem_u32(&mbar), (uint32_t)((count - 1) & 1));
-    if (__syncthreads_or(!done)) {
-      ok = false;
-      if (tid == 0) atomicExch(&g_tc_error, 1);
-    } else {
-      tc_fence_after();
-      cp_async_wait<0>();
-      __syncthreads();
-      epilogue(count - 1, raw);
+      tc_commit(smem_u32(&bar_mma[j & 1]));
     }
   }
-  cp_async_wait<0>();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -383,7 +445,6 @@ template <int KQ>
 void launch_tc(const State& st, const Pass& p, const void* b_image) {
   using Cfg = TcCfg<KQ>;
   TcGeom g{};
-  g.tb = Cfg::TB;
   uint64_t tmask = 0;
   for (int b = 0; b < p.k; ++b) tmask |= uint64_t{1} << p.qubits[b];
   uint64_t tiles_mask = tmask;
@@ -401,6 +462,10 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
       g.is_target[j] = (int)((tmask >> q) & 1);
       ++j;
     }
+  g.m_low = 0;
+  while (g.m_low < Cfg::TB && g.tile_pos[g.m_low] == g.m_low) ++g.m_low;
+  g.nh = 0;
+  for (int i = g.m_low; i < Cfg::TB; ++i) g.hpos[g.nh++] = g.tile_pos[i];
   g.n_tiles = st.dim() >> Cfg::TB;
   static int attr_done[64] = {0};
   if (st.device >= 0 && st.device < 64 && !(attr_done[st.device] & (1 << KQ))) {
@@ -456,6 +521,7 @@ void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& 
       const float l = f - hf;
       uint32_t lu;
       std::memcpy(&lu, &l, 4);
+      lu = host_tf32_rna(l);  // unbiased: the tensor core would truncate it
       const uint32_t off = sw128_offset(n, kk, N);
       std::memcpy(hi + off, &h, 4);
       std::memcpy(lo + off, &lu, 4);

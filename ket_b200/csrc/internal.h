@@ -134,6 +134,7 @@ bool tc_supported(int k);
 void set_ground(const State& s);
 double reduce_norm(const State& s);
 cplx reduce_inner(const State& a, const State& b);
+void compare_states(const State& a, const State& b, double out[5]);
 void expval_terms(const State& s, const std::vector<uint64_t>& flip,
                   const std::vector<uint64_t>& sign, const std::vector<int>& phase,
                   double* out);

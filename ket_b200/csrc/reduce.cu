@@ -13,6 +13,7 @@
 // block partials reduced in index order by a second kernel.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -90,6 +91,42 @@ __global__ void inner_partial(const T* __restrict__ a, const T* __restrict__ b, 
   if (threadIdx.x == 0) {
     part[2 * blockIdx.x] = r0;
     part[2 * blockIdx.x + 1] = r1;
+  }
+}
+
+// Mixed-precision comparison: max |a-b| and the sums <a|b>, <a|a>, <b|b>.
+template <typename TA, typename TB>
+__global__ void compare_partial(const TA* __restrict__ a, const TB* __restrict__ b, uint64_t dim,
+                                double* __restrict__ part /* 5 per block */) {
+  __shared__ double sh[32];
+  double re = 0, im = 0, na = 0, nb = 0, mx = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < dim;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const TA u = a[i];
+    const TB v = b[i];
+    const double ur = AmpT<TA>::re(u), ui = AmpT<TA>::im(u);
+    const double vr = AmpT<TB>::re(v), vi = AmpT<TB>::im(v);
+    re += ur * vr + ui * vi;
+    im += ur * vi - ui * vr;
+    na += ur * ur + ui * ui;
+    nb += vr * vr + vi * vi;
+    mx = fmax(mx, fmax(fabs(ur - vr), fabs(ui - vi)));
+  }
+  const double r0 = block_sum(re, sh), r1 = block_sum(im, sh), r2 = block_sum(na, sh), r3 = block_sum(nb, sh);
+  // block max
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  if (lane == 0) sh[warp] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sh[w]);
+    part[5 * blockIdx.x + 0] = m;
+    part[5 * blockIdx.x + 1] = r0;
+    part[5 * blockIdx.x + 2] = r1;
+    part[5 * blockIdx.x + 3] = r2;
+    part[5 * blockIdx.x + 4] = r3;
   }
 }
 
@@ -357,6 +394,36 @@ cplx reduce_inner(const State& a, const State& b) {
   KB_CUDA(cudaMemcpyAsync(h, d + 2 * blocks, sizeof h, cudaMemcpyDeviceToHost, a.stream));
   KB_CUDA(cudaStreamSynchronize(a.stream));
   return {h[0], h[1]};
+}
+
+void compare_states(const State& a, const State& b, double out[5]) {
+  const int blocks = grid_for(a.dim(), kRThreads * 8);
+  Scratch part(sizeof(double) * 5 * blocks, a.stream);
+  double* d = part.as<double>();
+  KB_CUDA(cudaStreamSynchronize(b.stream));
+  const bool a64 = a.precision == KETGPU_C64, b64 = b.precision == KETGPU_C64;
+  if (a64 && b64)
+    compare_partial<float2, float2><<<blocks, kRThreads, 0, a.stream>>>(
+        static_cast<const float2*>(a.amps), static_cast<const float2*>(b.amps), a.dim(), d);
+  else if (a64)
+    compare_partial<float2, double2><<<blocks, kRThreads, 0, a.stream>>>(
+        static_cast<const float2*>(a.amps), static_cast<const double2*>(b.amps), a.dim(), d);
+  else if (b64)
+    compare_partial<double2, float2><<<blocks, kRThreads, 0, a.stream>>>(
+        static_cast<const double2*>(a.amps), static_cast<const float2*>(b.amps), a.dim(), d);
+  else
+    compare_partial<double2, double2><<<blocks, kRThreads, 0, a.stream>>>(
+        static_cast<const double2*>(a.amps), static_cast<const double2*>(b.amps), a.dim(), d);
+  count_launch();
+  KB_CUDA(cudaGetLastError());
+  std::vector<double> h((size_t)5 * blocks);
+  KB_CUDA(cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost, a.stream));
+  KB_CUDA(cudaStreamSynchronize(a.stream));
+  for (int w = 0; w < 5; ++w) out[w] = 0;
+  for (int bl = 0; bl < blocks; ++bl) {
+    out[0] = std::max(out[0], h[5 * bl]);
+    for (int w = 1; w < 5; ++w) out[w] += h[5 * bl + w];
+  }
 }
 
 void expval_terms(const State& st, const std::vector<uint64_t>& flip, const std::vector<uint64_t>& sign,
