@@ -28,6 +28,7 @@ thread_local std::string t_err;
 }
 
 void fail(int code, const std::string& msg) { throw Error(code, msg); }
+void set_last_error(const char* msg) { t_err = msg; }
 
 void check_cuda(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return;

@@ -267,7 +267,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   // sits at soff + 8 (qubit 0 is the lowest target: next combination) or at
   // soff + 8192 (qubit 0 is a group bit: row + 64).
   const uint32_t pair_step = q0_group ? 64u * 128u : 8u;
-  auto chunk_offsets = [&](int t, uint64_t* goff, uint32_t* soff) {
+  // Output staging when qubit 0 is a group bit: amplitudes e and e+1 (rows
+  // r and r+64, same combination c) side by side in one 16-byte slot, slot
+  // (r mod 64) * DIM + (c ^ (r mod 8)), so the store phase reads one 16-byte
+  // word per chunk and the TMEM drain writes stay spread over the banks.
+  auto pair_slot = [](int row, int comb) -> uint32_t {
+    return (uint32_t)(((row & 63) * Cfg::DIM + (comb ^ (row & 7))) * 16 + 8 * (row >> 6));
+  };
+  auto chunk_offsets = [&](int t, uint64_t* goff, uint32_t* soff, bool out_layout) {
 #pragma unroll
     for (int i = 0; i < CPT; ++i) {
       const int e = 2 * (t + kProducers * i);
@@ -281,7 +288,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
       const int row = q0_group ? ((grp >> 1) | ((grp & 1) << (kGroupBits - 1))) : grp;
       goff[i] = off;
-      soff[i] = sw128_offset(row, 2 * comb, 128);
+      soff[i] = (out_layout && q0_group) ? pair_slot(row, comb) : sw128_offset(row, 2 * comb, 128);
     }
   };
   auto tile_base = [&](uint64_t t) -> uint64_t {
@@ -297,7 +304,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ------------------------------------------------------------ producers
     uint64_t goff[CPT];
     uint32_t soff[CPT];
-    chunk_offsets(tid, goff, soff);
+    chunk_offsets(tid, goff, soff, false);
     for (uint64_t j = 0; j < count; ++j) {
       const int slot = (int)(j % S);
       if (j >= (uint64_t)S && !wait(&bar_free[slot], (uint32_t)(((j / S) - 1) & 1))) break;
@@ -366,7 +373,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int row = 32 * q + lane;
     uint64_t goff[CPT];
     uint32_t soff[CPT];
-    chunk_offsets(t, goff, soff);
+    chunk_offsets(t, goff, soff, true);
     for (uint64_t j = 0; j < count; ++j) {
       const int slot = (int)(j % S);
       if (!wait(&bar_mma[j & 1], (uint32_t)((j >> 1) & 1))) break;
@@ -379,28 +386,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
         tmem_ld<16>(acc + (uint32_t)(N + part * 16), vc);
         tmem_ld_wait();
+        if (q0_group) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-          *reinterpret_cast<float4*>(out + sw128_offset(row, part * 16 + 4 * i, 128)) =
-              make_float4(vm[4 * i] + vc[4 * i], vm[4 * i + 1] + vc[4 * i + 1], vm[4 * i + 2] + vc[4 * i + 2],
-                          vm[4 * i + 3] + vc[4 * i + 3]);
+          for (int i = 0; i < 8; ++i)
+            *reinterpret_cast<float2*>(out + pair_slot(row, part * 8 + i)) =
+                make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            *reinterpret_cast<float4*>(out + sw128_offset(row, part * 16 + 4 * i, 128)) =
+                make_float4(vm[4 * i] + vc[4 * i], vm[4 * i + 1] + vc[4 * i + 1], vm[4 * i + 2] + vc[4 * i + 2],
+                            vm[4 * i + 3] + vc[4 * i + 3]);
+        }
       }
       tc_fence_before();
       arrive(&bar_acc_free[j & 1]);
       asm volatile("bar.sync 1, %0;" ::"n"(kEpilogue) : "memory");
       float2* dst = s + base_ring[j % (2 * S)];
 #pragma unroll
-      for (int i = 0; i < CPT; ++i) {
-        float4 w;
-        if (q0_group) {
-          const float2 x = *reinterpret_cast<const float2*>(out + soff[i]);
-          const float2 y = *reinterpret_cast<const float2*>(out + soff[i] + pair_step);
-          w = make_float4(x.x, x.y, y.x, y.y);
-        } else {
-          w = *reinterpret_cast<const float4*>(out + soff[i]);
-        }
-        *reinterpret_cast<float4*>(dst + goff[i]) = w;
-      }
+      for (int i = 0; i < CPT; ++i)
+        *reinterpret_cast<float4*>(dst + goff[i]) = *reinterpret_cast<const float4*>(out + soff[i]);
       arrive(&bar_free[slot]);
     }
   } else if (warp == 12 && lane == 0) {

@@ -25,6 +25,7 @@ struct Error : std::runtime_error {
 };
 [[noreturn]] void fail(int code, const std::string& msg);
 void check_cuda(cudaError_t e, const char* what);
+void set_last_error(const char* msg);
 #define KB_CUDA(x) ::kb::check_cuda((x), #x)
 
 extern std::atomic<uint64_t> g_launches;

@@ -93,7 +93,9 @@ def qft_ghz_rz(n: int, seed: int = 7) -> Circuit:
 
 def variational_ansatz(n: int, layers: int) -> Tuple[Circuit, np.ndarray]:
     """Circuit with placeholder angles 0 and the parameter index of every op
-    (-1 for CX); parameters are ordered (layer, Ry for q=0..n-1, Rz q=0..n-1)."""
+    (-1 for CX and barriers); parameters are ordered (layer, Ry for
+    q=0..n-1, Rz for q=0..n-1).  A barrier closes each layer, which is what
+    the adjoint's checkpointing counts layers by."""
     c = Circuit(n)
     pidx: List[int] = []
     k = 0
@@ -109,6 +111,8 @@ def variational_ansatz(n: int, layers: int) -> Tuple[Circuit, np.ndarray]:
         for q in range(n):
             c.cx(q, (q + 1) % n)
             pidx.append(-1)
+        c.barrier()
+        pidx.append(-1)
     return c, np.array(pidx, dtype=np.int32)
 
 

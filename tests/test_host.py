@@ -122,7 +122,7 @@ def test_workload_shapes():
     c = qft_ghz_rz(33)
     assert len(c.gates) == 33 + 528 + 1 + 32 + 33
     a, pidx = variational_ansatz(24, 8)
-    assert (pidx >= 0).sum() == 384 and len(a.gates) == 8 * 72
+    assert (pidx >= 0).sum() == 384 and len(a.gates) == 8 * 73
     m = random_mixed(22, 20, seed=3)
     used = sum(len(g.qubits) for g in m.gates)
     assert used == 22 * 20
