@@ -210,14 +210,17 @@ int ketgpu_mlp_gradients(ketgpu_mlp* m, const float* x, const float* y,
 int ketgpu_mlp_train(ketgpu_mlp* m, const float* x, const float* y,
                      uint64_t n_samples, uint64_t steps, uint64_t minibatch,
                      float lr, float* final_loss);
-/* Attach a model to the learned planner (NULL detaches). */
+/* Attach a model to the learned planner (NULL detaches).  The model's
+ * output is log(pass time in microseconds). */
 int ketgpu_planner_set_model(ketgpu_mlp* m);
-/* The 48 features the planner scores a candidate block by. */
-int ketgpu_block_features(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
-                          const int32_t* block_qubits, int32_t k, float* out48);
-/* Time one dense k-qubit block pass on a state (microseconds, CUDA events). */
-int ketgpu_time_block(ketgpu_state* s, const int32_t* block_qubits, int32_t k,
-                      int32_t n_gates, int32_t reps, float* out_us);
+/* The 48 cost-model features of one pass applying `gates` on an
+ * n_qubits state: a dense block over the union of their qubits (fused = 1,
+ * tensor = 1 for the tcgen05 path) or one gate through its specialised
+ * kernel (fused = 0, exactly one gate). */
+int ketgpu_block_features(int32_t n_qubits, int32_t precision, const ketgpu_op* gates,
+                          uint64_t n_gates, int32_t fused, int32_t tensor, float* out48);
+/* The features of pass `index` of a plan (training rows for the model). */
+int ketgpu_plan_pass_features(const ketgpu_plan* p, uint64_t index, float* out48);
 
 #ifdef __cplusplus
 }

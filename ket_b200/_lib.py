@@ -96,8 +96,8 @@ def _load():
         "ketgpu_mlp_gradients": ([vp, vp, vp, u64] + [vp] * 7, ct.c_int),
         "ketgpu_mlp_train": ([vp, vp, vp, u64, u64, u64, ct.c_float, vp], ct.c_int),
         "ketgpu_planner_set_model": ([vp], ct.c_int),
-        "ketgpu_block_features": ([i32, vp, u64, vp, i32, vp], ct.c_int),
-        "ketgpu_time_block": ([vp, vp, i32, i32, i32, vp], ct.c_int),
+        "ketgpu_block_features": ([i32, i32, vp, u64, i32, i32, vp], ct.c_int),
+        "ketgpu_plan_pass_features": ([vp, u64, vp], ct.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -596,3 +596,21 @@ KB_API int ketgpu_compare(const ketgpu_state* a, const ketgpu_state* b, double* 
     compare_states(*as_state(a), *as_state(b), out5);
   });
 }
+
+KB_API int ketgpu_plan_pass_features(const ketgpu_plan* p, uint64_t index, float* out48) {
+  return guard([&] {
+    need(p && out48, "null argument");
+    const Plan& plan = *as_plan(p);
+    if (index >= plan.passes.size()) fail(KETGPU_ERR_OUT_OF_RANGE, "pass index out of range");
+    const Pass& ps = plan.passes[index];
+    std::vector<const ketgpu_op*> gs;
+    std::vector<int> qs;
+    for (int gi : ps.gates) {
+      gs.push_back(&plan.ops[gi]);
+      for (int j = 0; j < gate_arity(plan.ops[gi].type); ++j)
+        if (std::find(qs.begin(), qs.end(), plan.ops[gi].q[j]) == qs.end()) qs.push_back(plan.ops[gi].q[j]);
+    }
+    const bool fused = ps.kind == PassKind::Fused || ps.gates.size() > 1;
+    pass_features(plan.n, plan.precision, gs, qs, fused, ps.tensor, out48);
+  });
+}

@@ -72,12 +72,14 @@ struct Pass {
   size_t mat_index = 0;                // into Plan::matrices
   bool tensor = false;                 // tcgen05 path
   int first_op = 0, n_gates = 0;       // provenance
+  std::vector<int> gates;              // op indices of the gates this pass applies
   double bytes(int n, size_t amp) const;
 };
 
 struct Plan {
   int n = 0;
   int precision = KETGPU_C64;
+  std::vector<ketgpu_op> ops;  // the circuit the plan was built from
   std::vector<Pass> passes;
   std::vector<std::vector<cplx>> matrices;  // FP64 block matrices (host)
   // device copies, built lazily per device: FP64 (c128 SIMT), FP32 (c64 SIMT),
@@ -116,12 +118,15 @@ struct PlanOptions {
 PlanOptions resolve_options(const ketgpu_options* opt);
 void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops,
                 const PlanOptions& o);
-// Learned-planner hook (mlp.cu): score of a candidate block, microseconds.
+// Cost-model features of one pass: a dense block over `qubits` (fused) or
+// one gate through its specialised kernel (gates.size() == 1, !fused).
+constexpr int kFeatures = 48;
+void pass_features(int n, int precision, const std::vector<const ketgpu_op*>& gates,
+                   const std::vector<int>& qubits, bool fused, bool tensor, float* out);
+// Learned-planner hooks (mlp.cu): the attached model, and batched
+// predictions of pass times (microseconds) for feature rows.
 bool learned_model_attached();
-float learned_block_cost(int n, const std::vector<const ketgpu_op*>& gates,
-                         const int* qubits, int k);
-void block_features(int n, const std::vector<const ketgpu_op*>& gates,
-                    const int* qubits, int k, float* out48);
+void learned_predict(const std::vector<float>& rows, std::vector<float>& us);
 
 // ---- kernel launchers (gates.cu / fused_tc.cu / reduce.cu) -----------------
 void launch_pass(const State& s, const Plan& plan, const Pass& p);

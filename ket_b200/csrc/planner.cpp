@@ -248,7 +248,11 @@ double fused_cost_static(int k, int precision, bool tensor) {
   return k <= 4 ? 1.0 : (k == 5 ? 1.45 : 2.9);
 }
 
-// Greedy DAG-aware block growth over gates [lo, hi) of `ops`.
+bool block_on_tensor_cores(int n, int k, const PlanOptions& opt) {
+  return opt.precision == KETGPU_C64 && opt.tensor && tc_supported(k) && n >= k + 7;
+}
+
+// Greedy DAG-aware block growth over the gates `order` of `ops`.
 std::vector<Block> grow_blocks(int n, const ketgpu_op* ops, const std::vector<int>& order, int max_k) {
   std::vector<Block> blocks;
   std::vector<char> done(order.size(), 0);
@@ -333,6 +337,7 @@ void emit_single(Plan& plan, const ketgpu_op& o, int idx) {
   Pass p = lower_gate(o);
   p.first_op = idx;
   p.n_gates = 1;
+  p.gates = {idx};
   plan.passes.push_back(p);
 }
 
@@ -346,6 +351,7 @@ void emit_fused(Plan& plan, int n, const ketgpu_op* ops, const Block& b, const P
   Pass p;
   p.first_op = b.gates.front();
   p.n_gates = (int)b.gates.size();
+  p.gates = b.gates;
   if (k == 1) {  // one 2x2 through the streaming pair kernel
     p.kind = PassKind::Pair;
     p.mode = kPairGeneral;
@@ -360,7 +366,7 @@ void emit_fused(Plan& plan, int n, const ketgpu_op* ops, const Block& b, const P
   p.kind = PassKind::Fused;
   p.k = k;
   for (int j = 0; j < k; ++j) p.qubits[j] = qs[j];
-  p.tensor = opt.precision == KETGPU_C64 && opt.tensor && tc_supported(k) && n >= k + 7;
+  p.tensor = block_on_tensor_cores(n, k, opt);
   p.mat_index = plan.matrices.size();
   plan.matrices.push_back(std::move(mat));
   plan.passes.push_back(p);
@@ -368,9 +374,74 @@ void emit_fused(Plan& plan, int n, const ketgpu_op* ops, const Block& b, const P
 
 }  // namespace
 
+// 48 features: scale (n, bytes), pass kind, block geometry (k, span, low /
+// high qubits, runs of adjacent qubits, coalescing), gate content (counts by
+// kind), precision and an L2-residency flag.  Index layout is fixed; the
+// trained cost model depends on it.
+void pass_features(int n, int precision, const std::vector<const ketgpu_op*>& gates,
+                   const std::vector<int>& qubits, bool fused, bool tensor, float* f) {
+  for (int i = 0; i < kFeatures; ++i) f[i] = 0.f;
+  const double amp = precision == KETGPU_C64 ? 8.0 : 16.0;
+  const double state = amp * std::ldexp(1.0, n);
+  double frac = 1.0;
+  if (!fused && gates.size() == 1) frac = gate_traffic_fraction(*gates[0]);
+  const int k = (int)qubits.size();
+  int lo = n, hi = -1, runs = 0, low7 = 0;
+  std::vector<int> qs = qubits;
+  std::sort(qs.begin(), qs.end());
+  for (size_t i = 0; i < qs.size(); ++i) {
+    lo = std::min(lo, qs[i]);
+    hi = std::max(hi, qs[i]);
+    if (i == 0 || qs[i] != qs[i - 1] + 1) ++runs;
+    if (qs[i] < 7) ++low7;
+  }
+  f[0] = (float)n / 32.f;
+  f[1] = (float)(std::log2(2.0 * state * frac) / 40.0);
+  f[2] = fused ? 1.f : 0.f;
+  f[3] = tensor ? 1.f : 0.f;
+  f[4] = (float)k / 6.f;
+  f[5] = (float)gates.size() / 64.f;
+  f[6] = k ? (float)lo / (float)n : 0.f;
+  f[7] = k ? (float)hi / (float)n : 0.f;
+  f[8] = k ? (float)(hi - lo + 1) / (float)n : 0.f;
+  f[9] = (k && lo == 0) ? 1.f : 0.f;
+  f[10] = (float)low7 / 6.f;
+  f[11] = (float)runs / 6.f;
+  f[12] = (float)frac;
+  f[13] = precision == KETGPU_C128 ? 1.f : 0.f;
+  if (k >= 1 && k <= 6) f[13 + k] = 1.f;  // 14..19
+  for (const ketgpu_op* g : gates) {
+    int slot;
+    switch (g->type) {
+      case KETGPU_H: slot = 0; break;
+      case KETGPU_S: case KETGPU_SDG: case KETGPU_Z: case KETGPU_T: case KETGPU_TDG: slot = 1; break;
+      case KETGPU_RX: slot = 2; break;
+      case KETGPU_RY: slot = 3; break;
+      case KETGPU_RZ: slot = 4; break;
+      case KETGPU_U: case KETGPU_X: case KETGPU_Y: slot = 5; break;
+      case KETGPU_CX: case KETGPU_CY: slot = 6; break;
+      case KETGPU_CZ: slot = 7; break;
+      case KETGPU_CP: slot = 8; break;
+      case KETGPU_CRX: case KETGPU_CRY: case KETGPU_CRZ: case KETGPU_CU: case KETGPU_CH: slot = 9; break;
+      case KETGPU_SWAP: slot = 10; break;
+      case KETGPU_CCX: slot = 11; break;
+      case KETGPU_CSWAP: slot = 12; break;
+      default: slot = 13; break;
+    }
+    f[20 + slot] += 1.f / 16.f;  // 20..33
+  }
+  for (int q : qs) {
+    if (q < 8) f[34 + q] = 1.f;                    // 34..41
+    if (q >= n - 4) f[42 + (n - 1 - q)] = 1.f;      // 42..45
+  }
+  f[46] = state <= 126e6 ? 1.f : 0.f;
+  f[47] = 1.f;
+}
+
 void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const PlanOptions& opt) {
   plan.n = n;
   plan.precision = opt.precision;
+  plan.ops.assign(ops, ops + nops);
   plan.passes.clear();
   plan.matrices.clear();
   uint64_t n_gates = 0;
@@ -387,8 +458,63 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
         if (b.gates.size() == 1) emit_single(plan, ops[b.gates[0]], b.gates[0]);
         else emit_fused(plan, n, ops, b, opt);
       }
+    } else if (opt.fusion == KETGPU_FUSE_LEARNED && learned_model_attached()) {
+      // Candidate partitions (greedy growth at k = 3..6); every block scored
+      // fused and as its separate gates by the cost model in one batched
+      // inference; the partition with the least predicted time wins, each
+      // block taking its cheaper form.
+      const int kmax_cap = std::max(2, std::min(6, opt.max_k + 1));
+      std::vector<std::vector<Block>> cands;
+      for (int kc = 3; kc <= kmax_cap; ++kc) cands.push_back(grow_blocks(n, ops, seg, kc));
+      std::vector<float> rows;
+      float fr[kFeatures];
+      // single-gate rows, one per gate of the segment
+      std::vector<size_t> single_row(nops, 0);
+      for (int gi : seg) {
+        std::vector<int> q1(ops[gi].q, ops[gi].q + gate_arity(ops[gi].type));
+        pass_features(n, opt.precision, {&ops[gi]}, q1, false, false, fr);
+        single_row[gi] = rows.size() / kFeatures;
+        rows.insert(rows.end(), fr, fr + kFeatures);
+      }
+      std::vector<std::vector<size_t>> fused_row(cands.size());
+      for (size_t c = 0; c < cands.size(); ++c)
+        for (const Block& b : cands[c]) {
+          std::vector<const ketgpu_op*> gs;
+          for (int gi : b.gates) gs.push_back(&ops[gi]);
+          pass_features(n, opt.precision, gs, b.qubits, true,
+                        block_on_tensor_cores(n, (int)b.qubits.size(), opt), fr);
+          fused_row[c].push_back(rows.size() / kFeatures);
+          rows.insert(rows.end(), fr, fr + kFeatures);
+        }
+      std::vector<float> us;
+      learned_predict(rows, us);
+      size_t best = 0;
+      double best_t = 1e300;
+      std::vector<std::vector<char>> choice(cands.size());
+      for (size_t c = 0; c < cands.size(); ++c) {
+        double tot = 0;
+        for (size_t bi = 0; bi < cands[c].size(); ++bi) {
+          const Block& b = cands[c][bi];
+          double sep = 0;
+          for (int gi : b.gates) sep += us[single_row[gi]];
+          const double fu = us[fused_row[c][bi]];
+          const bool fuse = b.gates.size() > 1 && fu < sep;
+          choice[c].push_back(fuse ? 1 : 0);
+          tot += fuse ? fu : sep;
+        }
+        if (tot < best_t) {
+          best_t = tot;
+          best = c;
+        }
+      }
+      predicted += best_t;
+      for (size_t bi = 0; bi < cands[best].size(); ++bi) {
+        const Block& b = cands[best][bi];
+        if (choice[best][bi]) emit_fused(plan, n, ops, b, opt);
+        else
+          for (int gi : b.gates) emit_single(plan, ops[gi], gi);
+      }
     } else {
-      const bool learned = opt.fusion == KETGPU_FUSE_LEARNED && learned_model_attached();
       for (const Block& b : grow_blocks(n, ops, seg, std::max(1, opt.max_k))) {
         if (b.gates.size() == 1) {
           emit_single(plan, ops[b.gates[0]], b.gates[0]);
@@ -397,26 +523,7 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
         const int k = (int)b.qubits.size();
         double separate = 0;
         for (int gi : b.gates) separate += gate_traffic_fraction(ops[gi]);
-        bool fuse;
-        if (learned) {
-          std::vector<const ketgpu_op*> gs;
-          for (int gi : b.gates) gs.push_back(&ops[gi]);
-          std::vector<int> qs = b.qubits;
-          const float fused_us = learned_block_cost(n, gs, qs.data(), k);
-          double sep_us = 0;
-          for (int gi : b.gates) {
-            std::vector<const ketgpu_op*> one{&ops[gi]};
-            std::vector<int> q1;
-            for (int j = 0; j < gate_arity(ops[gi].type); ++j) q1.push_back(ops[gi].q[j]);
-            std::sort(q1.begin(), q1.end());
-            sep_us += learned_block_cost(n, one, q1.data(), (int)q1.size());
-          }
-          fuse = fused_us < sep_us;
-          predicted += fuse ? fused_us : sep_us;
-        } else {
-          fuse = fused_cost_static(k, opt.precision, opt.tensor) < separate;
-        }
-        if (fuse) {
+        if (fused_cost_static(k, opt.precision, opt.tensor) < separate) {
           emit_fused(plan, n, ops, b, opt);
         } else {
           for (int gi : b.gates) emit_single(plan, ops[gi], gi);
