@@ -77,6 +77,9 @@ typedef struct ketgpu_options {
   int32_t fusion;           /* ketgpu_fusion */
   int32_t max_block_qubits; /* k <= 6 (fused blocks); 0 = default (5) */
   int32_t tensor_cores;     /* 1: complex64 blocks on tcgen05 (3xTF32); 0: SIMT */
+  int32_t renormalize;      /* 0: restore the starting norm after tensor-core
+                               blocks (their FP32 accumulation rounds toward
+                               zero); -1: never; 1: after every plan */
 } ketgpu_options;
 
 typedef struct ketgpu_plan_stats {
@@ -110,6 +113,9 @@ void* ketgpu_state_device_ptr(const ketgpu_state* s);
 /* Copy amplitudes [first, first+count) to a host complex128 buffer. */
 int ketgpu_state_download(const ketgpu_state* s, uint64_t first, uint64_t count,
                           double* out_c128);
+/* Copy amplitudes [first, first+count) to a host buffer in the state's own
+ * format (complex64 or complex128 interleaved), without conversion. */
+int ketgpu_state_download_raw(const ketgpu_state* s, uint64_t first, uint64_t count, void* out);
 /* Overwrite amplitudes [first, first+count) from a host complex128 buffer. */
 int ketgpu_state_upload(ketgpu_state* s, uint64_t first, uint64_t count,
                         const double* in_c128);

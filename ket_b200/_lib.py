@@ -31,7 +31,8 @@ assert OP_DTYPE.itemsize == 48
 
 class Options(ct.Structure):
     _fields_ = [("precision", ct.c_int32), ("fusion", ct.c_int32),
-                ("max_block_qubits", ct.c_int32), ("tensor_cores", ct.c_int32)]
+                ("max_block_qubits", ct.c_int32), ("tensor_cores", ct.c_int32),
+                ("renormalize", ct.c_int32)]
 
 
 class PlanStats(ct.Structure):
@@ -67,6 +68,7 @@ def _load():
         "ketgpu_state_device_ptr": ([vp], vp),
         "ketgpu_state_download": ([vp, u64, u64, vp], ct.c_int),
         "ketgpu_state_upload": ([vp, u64, u64, vp], ct.c_int),
+        "ketgpu_state_download_raw": ([vp, u64, u64, vp], ct.c_int),
         "ketgpu_state_copy": ([vp, vp], ct.c_int),
         "ketgpu_state_synchronize": ([vp], ct.c_int),
         "ketgpu_plan_create": ([i32, vp, u64, ct.POINTER(Options), ct.POINTER(vp)], ct.c_int),

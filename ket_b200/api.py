@@ -25,7 +25,7 @@ _PRECISIONS = {"c64": C64, "complex64": C64, "c128": C128, "complex128": C128}
 _FUSIONS = {"none": FUSE_NONE, "unfused": FUSE_NONE, "reference": FUSE_REFERENCE,
             "greedy": FUSE_GREEDY, "learned": FUSE_LEARNED}
 
-_opts = _lib.Options(C128, FUSE_GREEDY, 5, 1)
+_opts = _lib.Options(C128, FUSE_GREEDY, 5, 1, 0)
 _num_threads = [1]
 
 
@@ -48,10 +48,13 @@ def get_options() -> dict:
             "max_block_qubits": _opts.max_block_qubits, "tensor_cores": bool(_opts.tensor_cores)}
 
 
-def make_options(precision="c128", fusion="greedy", max_block_qubits=5, tensor_cores=True) -> _lib.Options:
+def make_options(precision="c128", fusion="greedy", max_block_qubits=5, tensor_cores=True,
+                 renormalize=0) -> _lib.Options:
+    """renormalize: 0 restores the starting norm after tensor-core blocks,
+    -1 never, 1 after every plan."""
     return _lib.Options(_PRECISIONS[precision] if isinstance(precision, str) else int(precision),
                         _FUSIONS[fusion] if isinstance(fusion, str) else int(fusion),
-                        int(max_block_qubits), 1 if tensor_cores else 0)
+                        int(max_block_qubits), 1 if tensor_cores else 0, int(renormalize))
 
 
 def set_num_threads(threads: int) -> None:
@@ -101,7 +104,7 @@ class DeviceState:
 
     def apply(self, circuit: Union[Circuit, np.ndarray], options: Optional[_lib.Options] = None):
         ops = circuit.to_ops() if isinstance(circuit, Circuit) else np.ascontiguousarray(circuit)
-        opt = options or _lib.Options(self.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores)
+        opt = options or _lib.Options(self.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores, 0)
         check(lib.ketgpu_apply(self._h, ops.ctypes.data, len(ops), ct.byref(opt)))
         return self
 
@@ -110,6 +113,14 @@ class DeviceState:
         count = dim - first if count is None else count
         out = np.empty(count, dtype=np.complex128)
         check(lib.ketgpu_state_download(self._h, first, count, out.ctypes.data))
+        return out
+
+    def to_numpy_raw(self, first: int = 0, count: Optional[int] = None) -> np.ndarray:
+        """Amplitudes in the state's own precision (complex64 or complex128)."""
+        dim = 1 << self.n_qubits
+        count = dim - first if count is None else count
+        out = np.empty(count, dtype=np.complex64 if self.precision == C64 else np.complex128)
+        check(lib.ketgpu_state_download_raw(self._h, first, count, out.ctypes.data))
         return out
 
     def from_numpy(self, amps: np.ndarray, first: int = 0):
@@ -207,7 +218,7 @@ class ProbeRun:
 # ---------------------------------------------------------------------------
 def run_device(circuit: Circuit, precision=None, options: Optional[_lib.Options] = None) -> DeviceState:
     """Evolve |0...0> on the GPU and keep the state there."""
-    opt = options or _lib.Options(_opts.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores)
+    opt = options or _lib.Options(_opts.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores, 0)
     if precision is not None:
         opt.precision = _PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     d = DeviceState(circuit.n_qubits, opt.precision)
@@ -387,7 +398,7 @@ def sample_shots(circuit: Circuit, shots: int, seed: int = 0) -> np.ndarray:
 
 def plan_stats(circuit: Circuit, options: Optional[_lib.Options] = None) -> dict:
     ops = circuit.to_ops()
-    opt = options or _lib.Options(_opts.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores)
+    opt = options or _lib.Options(_opts.precision, _opts.fusion, _opts.max_block_qubits, _opts.tensor_cores, 0)
     h = ct.c_void_p()
     check(lib.ketgpu_plan_create(circuit.n_qubits, ops.ctypes.data, len(ops), ct.byref(opt), ct.byref(h)))
     st = _lib.PlanStats()

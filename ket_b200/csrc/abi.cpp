@@ -53,6 +53,7 @@ Plan::~Plan() {
     if (d_mat64) cudaFree(d_mat64);
     if (d_mat32) cudaFree(d_mat32);
     if (d_tc) cudaFree(d_tc);
+    if (d_norm) cudaFree(d_norm);
     if (prev >= 0) cudaSetDevice(prev);
   }
 }
@@ -84,6 +85,9 @@ void upload_plan_matrices(Plan& plan, int device) {
   if (plan.device == device) return;
   if (plan.device >= 0) fail(KETGPU_ERR_INVALID, "plan was prepared for another device");
   plan.device = device;
+  for (const Pass& p : plan.passes)
+    if (p.kind == PassKind::NormCapture && !plan.d_norm)
+      KB_CUDA(cudaMalloc(&plan.d_norm, sizeof(double) * (2 + kNormBlocks)));
   if (plan.matrices.empty()) return;
   std::vector<double> h64;
   std::vector<float> h32;
@@ -355,6 +359,20 @@ KB_API int ketgpu_state_download(const ketgpu_state* s, uint64_t first, uint64_t
   });
 }
 
+KB_API int ketgpu_state_download_raw(const ketgpu_state* s, uint64_t first, uint64_t count, void* out) {
+  return guard([&] {
+    need(s != nullptr && (out != nullptr || count == 0), "null argument");
+    const State& st = *as_state(s);
+    if (first > st.dim() || count > st.dim() - first)
+      fail(KETGPU_ERR_OUT_OF_RANGE, "amplitude range outside the state");
+    DeviceGuard g(st.device);
+    const size_t b = st.amp_bytes();
+    KB_CUDA(cudaMemcpyAsync(out, static_cast<const char*>(st.amps) + first * b, count * b, cudaMemcpyDeviceToHost,
+                            st.stream));
+    KB_CUDA(cudaStreamSynchronize(st.stream));
+  });
+}
+
 KB_API int ketgpu_state_upload(ketgpu_state* s, uint64_t first, uint64_t count, const double* in) {
   return guard([&] {
     need(s != nullptr && (in != nullptr || count == 0), "null argument");
@@ -577,7 +595,8 @@ KB_API int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* 
     const Plan& plan = *as_plan(p);
     if (index >= plan.passes.size()) fail(KETGPU_ERR_OUT_OF_RANGE, "pass index out of range");
     const Pass& ps = plan.passes[index];
-    if (kind) *kind = ps.kind == PassKind::Pair ? 0 : ps.kind == PassKind::Phase ? 1 : 2;
+    if (kind)
+      *kind = ps.kind == PassKind::Pair ? 0 : ps.kind == PassKind::Phase ? 1 : ps.kind == PassKind::Fused ? 2 : 3;
     if (k) *k = ps.kind == PassKind::Fused ? ps.k : ps.nfixed;
     if (tensor) *tensor = ps.tensor ? 1 : 0;
     if (bytes) *bytes = ps.bytes(plan.n, plan.precision == KETGPU_C64 ? 8 : 16);

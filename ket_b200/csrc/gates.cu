@@ -322,6 +322,8 @@ void launch_fused_simt(const State& st, const Pass& p, const void* mat_t) {
 double Pass::bytes(int n, size_t amp) const {
   const double dim = (double)(uint64_t{1} << n);
   if (kind == PassKind::Fused) return 2.0 * amp * dim;
+  if (kind == PassKind::NormCapture) return amp * dim;
+  if (kind == PassKind::NormRestore) return 3.0 * amp * dim;
   if (kind == PassKind::Phase) return 2.0 * amp * dim / (double)(uint64_t{1} << nfixed);
   // pair: two amplitudes per pair, both read and written
   return 2.0 * amp * 2.0 * dim / (double)(uint64_t{1} << nfixed);
@@ -338,6 +340,15 @@ void set_ground(const State& s) {
 }
 
 void launch_pass(const State& s, const Plan& plan, const Pass& p) {
+  if (p.kind == PassKind::NormCapture) {
+    norm_to_device(s, plan.d_norm + 2, plan.d_norm);
+    return;
+  }
+  if (p.kind == PassKind::NormRestore) {
+    norm_to_device(s, plan.d_norm + 2, plan.d_norm + 1);
+    rescale_state(s, plan.d_norm, plan.d_norm + 1);
+    return;
+  }
   if (p.kind != PassKind::Fused) {
     if (s.precision == KETGPU_C64)
       launch_pair<float>(s, p);

@@ -56,6 +56,8 @@ enum class PassKind : int {
              // indices with zeros at the fixed positions
   Phase,     // multiply the amplitudes with all fixed bits set by a phase
   Fused,     // dense 2^k x 2^k complex matrix on k qubits
+  NormCapture,  // record the state's squared norm (FP64) on the device
+  NormRestore,  // rescale the state to the recorded squared norm
 };
 enum PairMode : int { kPairGeneral = 0, kPairSwap = 1, kPairDiag = 2 };
 
@@ -87,6 +89,7 @@ struct Plan {
   void* d_mat64 = nullptr;
   void* d_mat32 = nullptr;
   void* d_tc = nullptr;
+  double* d_norm = nullptr;  // [captured, current, block partials...]
   std::vector<size_t> off64, off32, offtc;
   int device = -1;
   ketgpu_plan_stats stats{};
@@ -114,7 +117,9 @@ struct PlanOptions {
   int fusion = KETGPU_FUSE_GREEDY;
   int max_k = 5;
   bool tensor = true;
+  int renormalize = 0;
 };
+constexpr int kNormBlocks = 592;  // 4 x 148 SMs
 PlanOptions resolve_options(const ketgpu_options* opt);
 void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops,
                 const PlanOptions& o);
@@ -138,6 +143,10 @@ void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& 
 bool tc_supported(int k);
 
 void set_ground(const State& s);
+// Squared norm into a device scalar (partials: kNormBlocks doubles).
+void norm_to_device(const State& s, double* partials, double* out);
+// s *= sqrt(target[0] / current[0]), factor read on the device.
+void rescale_state(const State& s, const double* target, const double* current);
 double reduce_norm(const State& s);
 cplx reduce_inner(const State& a, const State& b);
 void compare_states(const State& a, const State& b, double out[5]);

@@ -230,6 +230,7 @@ PlanOptions resolve_options(const ketgpu_options* opt) {
   o.max_k = opt->max_block_qubits ? opt->max_block_qubits : 5;
   if (o.max_k < 1 || o.max_k > 6) fail(KETGPU_ERR_INVALID, "max_block_qubits must be in [1, 6]");
   o.tensor = opt->tensor_cores != 0;
+  o.renormalize = opt->renormalize;
   return o;
 }
 
@@ -541,6 +542,15 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
     }
   }
   flush();
+  bool any_tensor = false;
+  for (const Pass& p : plan.passes) any_tensor |= p.tensor;
+  if ((opt.renormalize == 0 && any_tensor) || (opt.renormalize > 0 && !plan.passes.empty())) {
+    Pass cap, res;
+    cap.kind = PassKind::NormCapture;
+    res.kind = PassKind::NormRestore;
+    plan.passes.insert(plan.passes.begin(), cap);
+    plan.passes.push_back(res);
+  }
   ketgpu_plan_stats& st = plan.stats;
   st = ketgpu_plan_stats{};
   st.n_gates = n_gates;

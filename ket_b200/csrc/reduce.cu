@@ -357,7 +357,43 @@ struct Scratch {
   }
 };
 
+template <typename T>
+__global__ void rescale_kernel(T* __restrict__ s, uint64_t dim, const double* __restrict__ target,
+                               const double* __restrict__ current) {
+  const double c = current[0];
+  const double f = c > 0.0 ? sqrt(target[0] / c) : 1.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+    T v = s[i];
+    v.x = (decltype(v.x))(v.x * f);
+    v.y = (decltype(v.y))(v.y * f);
+    s[i] = v;
+  }
+}
+
 }  // namespace
+
+void norm_to_device(const State& st, double* partials, double* out) {
+  if (st.precision == KETGPU_C64)
+    norm_partial<float2><<<kNormBlocks, kRThreads, 0, st.stream>>>(static_cast<const float2*>(st.amps), st.dim(),
+                                                                   partials);
+  else
+    norm_partial<double2><<<kNormBlocks, kRThreads, 0, st.stream>>>(static_cast<const double2*>(st.amps), st.dim(),
+                                                                    partials);
+  finish_partials<<<1, kRThreads, 0, st.stream>>>(partials, kNormBlocks, 1, out);
+  count_launch(2);
+  KB_CUDA(cudaGetLastError());
+}
+
+void rescale_state(const State& st, const double* target, const double* current) {
+  if (st.precision == KETGPU_C64)
+    rescale_kernel<float2><<<kNormBlocks, kRThreads, 0, st.stream>>>(static_cast<float2*>(st.amps), st.dim(),
+                                                                     target, current);
+  else
+    rescale_kernel<double2><<<kNormBlocks, kRThreads, 0, st.stream>>>(static_cast<double2*>(st.amps), st.dim(),
+                                                                      target, current);
+  count_launch();
+  KB_CUDA(cudaGetLastError());
+}
 
 double reduce_norm(const State& st) {
   const int blocks = grid_for(st.dim(), kRThreads * 8);

@@ -522,8 +522,21 @@ static int cmp_ukey(const void* a, const void* b) {
   return (x > y) - (x < y);
 }
 
+static void measure_sequential_many_any(int n, const double* s, const float* s32, const double* u,
+                                        size_t count, uint64_t* out);
+
 void ko_measure_sequential_many(int n, const double* s, const double* u,
                                 size_t count, uint64_t* out) {
+  measure_sequential_many_any(n, s, NULL, u, count, out);
+}
+
+void ko_measure_sequential_many32(int n, const float* s32, const double* u,
+                                  size_t count, uint64_t* out) {
+  measure_sequential_many_any(n, NULL, s32, u, count, out);
+}
+
+static void measure_sequential_many_any(int n, const double* s, const float* s32, const double* u,
+                                        size_t count, uint64_t* out) {
   const size_t dim = (size_t)1 << n;
   ukey* keys = (ukey*)malloc(sizeof(ukey) * (count ? count : 1));
   for (size_t j = 0; j < count; ++j) {
@@ -534,7 +547,7 @@ void ko_measure_sequential_many(int n, const double* s, const double* u,
   double cum = 0.0;
   size_t j = 0;
   for (size_t i = 0; i < dim && j < count; ++i) {
-    cum += norm_at(s, NULL, i);
+    cum += norm_at(s, s32, i);
     while (j < count && keys[j].u < cum) out[keys[j++].idx] = i;
   }
   while (j < count) out[keys[j++].idx] = dim - 1;

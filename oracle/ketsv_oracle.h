@@ -83,6 +83,10 @@ uint64_t ko_measure_sequential(int n, const double* amps, double u);
 void ko_measure_sequential_many(int n, const double* amps, const double* u,
                                 size_t count, uint64_t* out);
 
+/* The same for a complex64 state (probabilities computed in FP64). */
+void ko_measure_sequential_many32(int n, const float* amps32, const double* u,
+                                  size_t count, uint64_t* out);
+
 /* std::mt19937{seed} followed by uniform_real_distribution<double>(0,1)
  * draws, restated from the published MT19937 and libstdc++'s
  * generate_canonical<double,53> (two 32-bit words per draw). */

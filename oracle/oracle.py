@@ -80,6 +80,7 @@ class Oracle:
         L.ko_measure_sequential.argtypes = [i32, vp, ct.c_double]
         L.ko_measure_sequential.restype = ct.c_uint64
         L.ko_measure_sequential_many.argtypes = [i32, vp, vp, sz, vp]
+        L.ko_measure_sequential_many32.argtypes = [i32, vp, vp, sz, vp]
         L.ko_uniforms_mt19937.argtypes = [ct.c_uint32, sz, vp]
         L.ko_sample_tree.argtypes = [i32, vp, vp, vp, sz, vp]
         L.ko_adjoint.argtypes = [i32, vp, sz, vp, vp, sz, vp, vp, sz, vp, vp]
@@ -144,10 +145,14 @@ class Oracle:
         return out
 
     def measure_sequential(self, n, state, u):
-        st = np.ascontiguousarray(state, dtype=np.complex128)
         u = np.ascontiguousarray(u, dtype=np.float64)
         out = np.zeros(len(u), dtype=np.uint64)
-        self.L.ko_measure_sequential_many(n, st.ctypes.data, u.ctypes.data, len(u), out.ctypes.data)
+        if state.dtype == np.complex64:
+            st = np.ascontiguousarray(state)
+            self.L.ko_measure_sequential_many32(n, st.ctypes.data, u.ctypes.data, len(u), out.ctypes.data)
+        else:
+            st = np.ascontiguousarray(state, dtype=np.complex128)
+            self.L.ko_measure_sequential_many(n, st.ctypes.data, u.ctypes.data, len(u), out.ctypes.data)
         return out
 
     def sample_tree(self, n, state, u):

@@ -1,0 +1,114 @@
+"""ket's own C++ API, unchanged, running on the B200 backend.
+
+oracle/_ref/libket_dropin.so is ket's off-path translation units (circuit,
+DAG, state, QASM, backend dispatch, stabilizer) linked with
+ket_b200/host/ket_statevector_gpu.cpp in place of ket's state-vector units;
+oracle/_ref/libket_ref.so is ket itself.  The same shim drives both through
+ket::run / expval / measure / sample / simulate, so every difference below
+is the backend's.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle import ARITY, DROPIN_SO, GATES, NPARAMS, REF_SO, make_ops
+
+pytestmark = pytest.mark.skipif(not (os.path.exists(REF_SO) and os.path.exists(DROPIN_SO)),
+                                reason="ket sources were not available to build the drop-in")
+
+
+def _libs():
+    from oracle.oracle import Reference
+    return Reference(dropin=False), Reference(dropin=True)
+
+
+def _random_ops(n, count, seed, gates=GATES[:24]):
+    rng = np.random.default_rng(seed)
+    gs = []
+    for _ in range(count):
+        g = gates[int(rng.integers(len(gates)))]
+        qs = rng.choice(n, ARITY[g], replace=False).tolist()
+        ps = rng.uniform(0, 2 * math.pi, NPARAMS.get(g, 0)).tolist()
+        gs.append((g, qs, ps))
+    return make_ops(gs)
+
+
+def test_dropin_library_loads_and_exports_the_shim():
+    import ctypes
+    lib = ctypes.CDLL(DROPIN_SO)
+    for name in ("ref_run", "ref_expval_sum", "ref_sample", "ref_simulate_sample", "ref_is_clifford"):
+        assert hasattr(lib, name)
+
+
+def test_routing_decisions_are_kets_own():
+    R, D = _libs()
+    cliff = make_ops([("H", [0]), ("CX", [0, 1]), ("S", [1]), ("Swap", [1, 2]), ("Measure", [0, 0])])
+    non = make_ops([("H", [0]), ("T", [0]), ("Measure", [0, 0])])
+    for ops in (cliff, non):
+        assert R.is_clifford(3, ops) == D.is_clifford(3, ops)
+        assert R.chosen_method(3, ops) == D.chosen_method(3, ops)
+
+
+@pytest.mark.gpu
+def test_run_matches_ket():
+    R, D = _libs()
+    for n, count, seed in [(3, 40, 1), (8, 200, 2), (12, 300, 3)]:
+        ops = _random_ops(n, count, seed)
+        assert np.abs(R.run(n, ops) - D.run(n, ops)).max() < 1e-12
+
+
+@pytest.mark.gpu
+def test_run_with_probes_matches_ket():
+    R, D = _libs()
+    ops = make_ops([("H", [0]), ("Probe", []), ("CX", [0, 1]), ("T", [1]), ("Probe", []), ("Rx", [2], [0.4])])
+    fr, pr = R.run_with_probes(3, ops)
+    fd, pd = D.run_with_probes(3, ops)
+    assert len(pr) == len(pd) == 2
+    assert np.abs(fr - fd).max() < 1e-12 and np.abs(pr - pd).max() < 1e-12
+
+
+@pytest.mark.gpu
+def test_expval_matches_ket():
+    R, D = _libs()
+    n = 9
+    ops = _random_ops(n, 150, 4)
+    st = R.run(n, ops)
+    g = np.random.default_rng(5)
+    terms = [(float(g.standard_normal()), "".join("IXYZ"[i] for i in g.integers(0, 4, n))) for _ in range(12)]
+    assert abs(R.expval_sum(n, st, terms) - D.expval_sum(n, st, terms)) < 1e-12
+    for _, p in terms[:4]:
+        assert abs(R.expval(n, st, p) - D.expval(n, st, p)) < 1e-12
+    for method in (0, 1):
+        assert abs(R.expval_circuit(n, ops, terms, method) - D.expval_circuit(n, ops, terms, method)) < 1e-12
+    with pytest.raises(ValueError):
+        D.expval(n, st, "ZZ")
+
+
+@pytest.mark.gpu
+def test_measure_and_sample_match_ket():
+    R, D = _libs()
+    n = 5
+    ops = _random_ops(n, 60, 6)
+    st = R.run(n, ops)
+    # n = 5 is a single 32-amplitude segment: the tree sampler is ket's scan
+    assert np.array_equal(R.measure(n, st, 42, 300), D.measure(n, st, 42, 300))
+    circ = np.concatenate([ops, make_ops([("Measure", [0, 0]), ("Measure", [3, 1]), ("Measure", [4, 2])])])
+    for method in (0, 1):
+        assert np.array_equal(R.sample(n, circ, 7, 50, method), D.sample(n, circ, 7, 50, method))
+    # one Simulation, many shots: the GPU backend answers from HBM
+    a, name_r = R.sample(n, circ, 9, 500, method=1, evolve_once=True)
+    b, name_d = D.sample(n, circ, 9, 500, method=1, evolve_once=True)
+    assert np.array_equal(a, b) and name_r == name_d == "state vector"
+
+
+@pytest.mark.gpu
+def test_clifford_circuits_stay_on_kets_stabilizer():
+    R, D = _libs()
+    ops = make_ops([("H", [0]), ("CX", [0, 1]), ("CX", [1, 2]), ("S", [2]), ("Measure", [0, 0]),
+                    ("Measure", [1, 1]), ("Measure", [2, 2])])
+    a, name_r = R.sample(3, ops, 11, 200, method=0, evolve_once=True)
+    b, name_d = D.sample(3, ops, 11, 200, method=0, evolve_once=True)
+    assert name_r == name_d == "stabilizer"
+    assert np.array_equal(a, b)
