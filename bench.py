@@ -118,33 +118,22 @@ def cpu_baseline_reference(circ_ops, seconds_budget=20.0):
 
 
 def init_dist(n_gpus):
-    rank, world, local = 0, 1, 0
+    """One process per GPU (torchrun); replicas share nothing but timings."""
+    from ket_b200 import replicas
     if n_gpus > 1 or "RANK" in os.environ:
-        import torch.distributed as dist
-        rank = int(os.environ.get("RANK", 0))
-        world = int(os.environ.get("WORLD_SIZE", 1))
-        local = int(os.environ.get("LOCAL_RANK", 0))
-        import datetime
-        import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    return rank, world, local
+        return replicas.init("nccl")
+    return 0, 1, 0
 
 
 def barrier_max(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from ket_b200 import replicas
+    return replicas.max_over_ranks(x, device="cuda") if world > 1 else x
 
 
 def barrier(world):
+    from ket_b200 import replicas
     if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        replicas.barrier()
 
 
 def run_reference_arm(args):

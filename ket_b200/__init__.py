@@ -6,7 +6,8 @@ of ket_b200/csrc.
 """
 from .api import (DeviceState, Plan, ProbeRun, State, chosen_method, expval, get_options,
                   is_clifford, make_options, measure, num_threads, plan_stats, run, run_device,
-                  run_with_probes, sample, sample_shots, set_num_threads, set_options, uniforms)
+                  run_with_probes, sample, sample_shots, set_num_threads, set_options, uniforms,
+                  use_learned_planner)
 from .circuit import Circuit, Gate, GateType
 from ._lib import launch_count
 
@@ -14,5 +15,5 @@ __all__ = [
     "Circuit", "DeviceState", "Gate", "GateType", "Plan", "ProbeRun", "State", "chosen_method",
     "expval", "get_options", "is_clifford", "launch_count", "make_options", "measure",
     "num_threads", "plan_stats", "run", "run_device", "run_with_probes", "sample", "sample_shots",
-    "set_num_threads", "set_options", "uniforms",
+    "set_num_threads", "set_options", "uniforms", "use_learned_planner",
 ]

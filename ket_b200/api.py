@@ -35,10 +35,26 @@ def set_options(precision=None, fusion=None, max_block_qubits=None, tensor_cores
         _opts.precision = _PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     if fusion is not None:
         _opts.fusion = _FUSIONS[fusion] if isinstance(fusion, str) else int(fusion)
+        if _opts.fusion == FUSE_LEARNED:
+            use_learned_planner()
     if max_block_qubits is not None:
         _opts.max_block_qubits = int(max_block_qubits)
     if tensor_cores is not None:
         _opts.tensor_cores = 1 if tensor_cores else 0
+
+
+_model = [None]
+
+
+def use_learned_planner(path: Optional[str] = None):
+    """Attach the trained cost model (ket_b200/data/cost_model.npz unless
+    `path` is given) to the planner's FUSE_LEARNED mode; returns it."""
+    from .planner import DEFAULT_MODEL, CostModel
+    if _model[0] is None or path is not None:
+        m = CostModel.load(path or DEFAULT_MODEL)
+        m.attach()
+        _model[0] = m
+    return _model[0]
 
 
 def get_options() -> dict:

@@ -128,6 +128,102 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
+// Vectorised complex64 forms.  When no fixed qubit is qubit 0, pair indices
+// 2t and 2t+1 own adjacent amplitudes, so one 16-byte load carries two
+// complex64 values per side of the pair; a 1-qubit gate on qubit 0 owns the
+// adjacent amplitudes (2i, 2i+1) themselves.
+
+__device__ __forceinline__ float2 cmul_add(float ar, float ai, float2 a, float br, float bi, float2 b) {
+  return make_float2(ar * a.x - ai * a.y + br * b.x - bi * b.y, ar * a.y + ai * a.x + br * b.y + bi * b.x);
+}
+
+template <int MODE>
+__device__ __forceinline__ void pair_update(const Mat2<float>& m, float2 a, float2 b, float2& x, float2& y) {
+  if (MODE == kPairSwap) {
+    x = b;
+    y = a;
+  } else if (MODE == kPairDiag) {
+    x = make_float2(m.re[0] * a.x - m.im[0] * a.y, m.re[0] * a.y + m.im[0] * a.x);
+    y = make_float2(m.re[3] * b.x - m.im[3] * b.y, m.re[3] * b.y + m.im[3] * b.x);
+  } else {
+    x = cmul_add(m.re[0], m.im[0], a, m.re[1], m.im[1], b);
+    y = cmul_add(m.re[2], m.im[2], a, m.re[3], m.im[3], b);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+    pair_kernel_v2(float2* __restrict__ s, PairGeom g, Mat2<float> m) {
+  const uint64_t count2 = g.count >> 1;
+  const uint64_t start = (uint64_t)blockIdx.x * (kThreads * kUnroll) + threadIdx.x;
+  float4 a[kUnroll], b[kUnroll];
+  uint64_t k0[kUnroll];
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    const uint64_t t = start + (uint64_t)u * kThreads;
+    k0[u] = ~uint64_t{0};
+    if (t < count2) {
+      k0[u] = spread(2 * t, g.fixed, g.nfixed);
+      a[u] = *reinterpret_cast<const float4*>(s + (k0[u] | g.p0));
+      b[u] = *reinterpret_cast<const float4*>(s + (k0[u] | g.p1));
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    if (k0[u] == ~uint64_t{0}) continue;
+    float2 x0, y0, x1, y1;
+    pair_update<MODE>(m, make_float2(a[u].x, a[u].y), make_float2(b[u].x, b[u].y), x0, y0);
+    pair_update<MODE>(m, make_float2(a[u].z, a[u].w), make_float2(b[u].z, b[u].w), x1, y1);
+    *reinterpret_cast<float4*>(s + (k0[u] | g.p0)) = make_float4(x0.x, x0.y, x1.x, x1.y);
+    *reinterpret_cast<float4*>(s + (k0[u] | g.p1)) = make_float4(y0.x, y0.y, y1.x, y1.y);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+    pair_kernel_q0(float2* __restrict__ s, uint64_t count, Mat2<float> m) {
+  const uint64_t start = (uint64_t)blockIdx.x * (kThreads * kUnroll) + threadIdx.x;
+  float4 v[kUnroll];
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    const uint64_t i = start + (uint64_t)u * kThreads;
+    if (i < count) v[u] = *reinterpret_cast<const float4*>(s + 2 * i);
+  }
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    const uint64_t i = start + (uint64_t)u * kThreads;
+    if (i >= count) continue;
+    float2 x, y;
+    pair_update<MODE>(m, make_float2(v[u].x, v[u].y), make_float2(v[u].z, v[u].w), x, y);
+    *reinterpret_cast<float4*>(s + 2 * i) = make_float4(x.x, x.y, y.x, y.y);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    phase_kernel_v2(float2* __restrict__ s, PairGeom g, float pre, float pim) {
+  const uint64_t count2 = g.count >> 1;
+  const uint64_t start = (uint64_t)blockIdx.x * (kThreads * kUnroll) + threadIdx.x;
+  float4 a[kUnroll];
+  uint64_t k[kUnroll];
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    const uint64_t t = start + (uint64_t)u * kThreads;
+    k[u] = ~uint64_t{0};
+    if (t < count2) {
+      k[u] = spread(2 * t, g.fixed, g.nfixed) | g.p0;
+      a[u] = *reinterpret_cast<const float4*>(s + k[u]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    if (k[u] == ~uint64_t{0}) continue;
+    const float4 x = a[u];
+    *reinterpret_cast<float4*>(s + k[u]) = make_float4(pre * x.x - pim * x.y, pre * x.y + pim * x.x,
+                                                       pre * x.z - pim * x.w, pre * x.w + pim * x.z);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Dense k-qubit block on CUDA cores (FP64 for complex128, FP32 for complex64
 // when the tensor-core path is off).  A CTA owns a tile of 2^TB amplitudes:
 // the k block qubits plus the lowest TB-k other qubits, so each of the 2^k
@@ -253,16 +349,51 @@ void launch_pair(const State& st, const Pass& p) {
   g.count = st.dim() >> p.nfixed;
   g.p0 = p.p0;
   g.p1 = p.p1;
-  const uint64_t blocks = (g.count + kThreads * kUnroll - 1) / (kThreads * kUnroll);
   T* s = static_cast<T*>(st.amps);
+  // complex64: 16-byte forms when the layout allows them
+  const bool vec2 = sizeof(R) == 4 && p.fixed[0] >= 1 && g.count >= 2;
+  const bool q0 = sizeof(R) == 4 && p.kind == PassKind::Pair && p.nfixed == 1 && p.fixed[0] == 0;
+  const uint64_t per_block = (uint64_t)kThreads * kUnroll;
+  const uint64_t blocks = ((vec2 ? g.count / 2 : g.count) + per_block - 1) / per_block;
+  Mat2<R> m;
+  for (int j = 0; j < 4; ++j) {
+    m.re[j] = (R)p.m[j].real();
+    m.im[j] = (R)p.m[j].imag();
+  }
   if (p.kind == PassKind::Phase) {
+    if constexpr (sizeof(R) == 4) {
+      if (vec2) {
+        phase_kernel_v2<<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g, (float)p.m[0].real(),
+                                                                      (float)p.m[0].imag());
+        count_launch();
+        KB_CUDA(cudaGetLastError());
+        return;
+      }
+    }
     phase_kernel<R><<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g, (R)p.m[0].real(),
                                                                   (R)p.m[0].imag());
   } else {
-    Mat2<R> m;
-    for (int j = 0; j < 4; ++j) {
-      m.re[j] = (R)p.m[j].real();
-      m.im[j] = (R)p.m[j].imag();
+    if constexpr (sizeof(R) == 4) {
+      if (vec2 || q0) {
+        if (vec2) {
+          if (p.mode == kPairSwap)
+            pair_kernel_v2<kPairSwap><<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g, m);
+          else if (p.mode == kPairDiag)
+            pair_kernel_v2<kPairDiag><<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g, m);
+          else
+            pair_kernel_v2<kPairGeneral><<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g, m);
+        } else {
+          if (p.mode == kPairSwap)
+            pair_kernel_q0<kPairSwap><<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g.count, m);
+          else if (p.mode == kPairDiag)
+            pair_kernel_q0<kPairDiag><<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g.count, m);
+          else
+            pair_kernel_q0<kPairGeneral><<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g.count, m);
+        }
+        count_launch();
+        KB_CUDA(cudaGetLastError());
+        return;
+      }
     }
     if (p.mode == kPairSwap)
       pair_kernel<R, kPairSwap><<<(unsigned)blocks, kThreads, 0, st.stream>>>(s, g, m);

@@ -126,3 +126,32 @@ def test_workload_shapes():
     m = random_mixed(22, 20, seed=3)
     used = sum(len(g.qubits) for g in m.gates)
     assert used == 22 * 20
+
+
+def test_cost_model_features_on_the_host():
+    import ctypes as ct
+    from ket_b200 import _lib
+    import ket_b200 as ket
+    c = ket.Circuit(20)
+    c.h(0)
+    c.cx(0, 5)
+    c.cp(5, 19, 0.3)
+    ops = c.to_ops()
+    f = np.zeros(48, dtype=np.float32)
+    _lib.check(_lib.lib.ketgpu_block_features(20, _lib.C64, ops.ctypes.data, len(ops), 1, 1, f.ctypes.data))
+    assert f[2] == 1 and f[3] == 1 and abs(f[4] - 3 / 6) < 1e-6 and f[47] == 1
+    assert f[34] == 1 and f[39] == 1 and f[42] == 1        # qubit 0, qubit 5, top qubit
+    assert abs(f[20] + f[6 + 20] + f[8 + 20] - 3 / 16) < 1e-6  # H, CX, CP counted
+    g = np.zeros(48, dtype=np.float32)
+    _lib.check(_lib.lib.ketgpu_block_features(20, _lib.C64, ops[2:].ctypes.data, 1, 0, 0, g.ctypes.data))
+    assert g[2] == 0 and abs(g[12] - 0.25) < 1e-6           # CP alone: a quarter of the state
+    assert _lib.lib.ketgpu_block_features(20, _lib.C64, ops.ctypes.data, 3, 0, 0, g.ctypes.data) == _lib.ERR_INVALID
+
+
+def test_learned_mode_without_a_model_falls_back_to_greedy():
+    import ket_b200 as ket
+    from ket_b200.workloads import random_mixed
+    c = random_mixed(24, 12, seed=4)
+    a = ket.plan_stats(c, ket.make_options("c64", "greedy", 5, True))
+    b = ket.plan_stats(c, ket.make_options("c64", "learned", 5, True))
+    assert a["n_passes"] == b["n_passes"] and a["bytes"] == b["bytes"]
