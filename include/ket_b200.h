@@ -163,6 +163,18 @@ int ketgpu_expval(const ketgpu_state* s, const char* pauli, double* out);
  * src/observable.cpp:85-91); every term in one batched reduction. */
 int ketgpu_expval_sum(const ketgpu_state* s, const double* coeffs,
                       const char* const* paulis, uint64_t n_terms, double* out);
+/* The value of ketgpu_expval_sum for callers that cannot allocate device
+ * memory during the call -- a service that keeps nearly all of HBM reserved
+ * for resident states, or code that must not have device memory allocated
+ * and freed underneath it.  No counterpart in ket (a variant of this
+ * backend's own ketgpu_expval_sum).  It uses a fixed scratch array of
+ * 608,256 bytes that every GPU loading the library holds until exit, shared
+ * by all calls (calls overlapping on one GPU race on it); the first call on a
+ * device looks the array up (make it before any stream capture).  At most
+ * KETGPU_NOALLOC_MAX_TERMS terms; more returns KETGPU_ERR_INVALID. */
+#define KETGPU_NOALLOC_MAX_TERMS 256
+int ketgpu_expval_sum_noalloc(const ketgpu_state* s, const double* coeffs,
+                              const char* const* paulis, uint64_t n_terms, double* out);
 /* Per-term expectations (out has n_terms entries). */
 int ketgpu_expval_terms(const ketgpu_state* s, const char* const* paulis,
                         uint64_t n_terms, double* out);

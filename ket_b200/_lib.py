@@ -86,6 +86,7 @@ def _load():
         "ketgpu_expval": ([vp, ct.c_char_p, pd], ct.c_int),
         "ketgpu_expval_sum": ([vp, vp, vp, u64, pd], ct.c_int),
         "ketgpu_expval_terms": ([vp, vp, u64, vp], ct.c_int),
+        "ketgpu_expval_sum_noalloc": ([vp, vp, vp, u64, pd], ct.c_int),
         "ketgpu_uniforms_mt19937": ([u32, u64, vp], ct.c_int),
         "ketgpu_sample": ([vp, vp, u64, vp], ct.c_int),
         "ketgpu_measure": ([vp, u32, ct.POINTER(u64)], ct.c_int),
