@@ -72,6 +72,8 @@ struct TcGeom {
   int m_low;          // tile qubits 0..m_low-1 form the low run
   int nh;             // tile qubits above the low run
   int hpos[16];
+  int direct;         // qubits 0..4 are group bits: the epilogue stores from registers
+  uint64_t cdep[32];  // offset of target combination c from its group's amplitude
   uint64_t n_tiles;
 };
 
@@ -335,8 +337,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ties away: magnitude bits plus half an ulp, truncated) and
     // lo = tf32(x - hi), and store both into the A region of tile parity j%2
     // in tensor memory once the MMAs of tile j-2 have released it.
+    // In the direct-store mode TMEM lane t carries group t (its staging row
+    // is the rotated one); otherwise lane t carries staging row t.
     const int q = warp & 3;
-    const int row = 32 * q + lane;
+    const int lane_row = 32 * q + lane;
+    const int row = g.direct ? ((lane_row >> 1) | ((lane_row & 1) << (kGroupBits - 1))) : lane_row;
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
     for (uint64_t j = 0; j < count; ++j) {
       const int slot = (int)(j % S);
@@ -365,12 +370,42 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       tc_fence_before();
       arrive(&bar_a_ready[j & 1]);
+      if (g.direct) arrive(&bar_free[slot]);  // nothing else reads this image
     }
   } else if (warp < 12) {
     // ------------------------------------------------------------- epilogue
     const int t = tid - 256;
     const int q = warp & 3;
     const int row = 32 * q + lane;
+    if (g.direct) {
+      // TMEM lane = group `row`; neighbouring lanes hold neighbouring
+      // amplitudes (qubits 0..4 are group bits), so each 8-byte store of a
+      // warp covers 256 contiguous bytes.
+      uint64_t gdep = 0;
+      for (int jb = 0, gb = 0; jb < Cfg::TB; ++jb)
+        if (!g.is_target[jb]) {
+          if ((row >> gb) & 1) gdep |= uint64_t{1} << g.tile_pos[jb];
+          ++gb;
+        }
+      for (uint64_t j = 0; j < count; ++j) {
+        if (!wait(&bar_mma[j & 1], (uint32_t)((j >> 1) & 1))) break;
+        tc_fence_after();
+        const uint32_t acc = tmem + (uint32_t)(2 * Cfg::A_COLS + (j & 1) * Cfg::ACC_COLS) + ((uint32_t)(32 * q) << 16);
+        float2* dst = s + base_ring[j % (2 * S)] + gdep;
+#pragma unroll
+        for (int part = 0; part < N / 16; ++part) {
+          float vm[16], vc[16];
+          tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
+          tmem_ld<16>(acc + (uint32_t)(N + part * 16), vc);
+          tmem_ld_wait();
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            dst[g.cdep[part * 8 + i]] = make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
+        }
+        tc_fence_before();
+        arrive(&bar_acc_free[j & 1]);
+      }
+    } else {
     uint64_t goff[CPT];
     uint32_t soff[CPT];
     chunk_offsets(t, goff, soff, true);
@@ -407,6 +442,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       for (int i = 0; i < CPT; ++i)
         *reinterpret_cast<float4*>(dst + goff[i]) = *reinterpret_cast<const float4*>(out + soff[i]);
       arrive(&bar_free[slot]);
+    }
     }
   } else if (warp == 12 && lane == 0) {
     // ------------------------------------------------------------ MMA issue
@@ -469,6 +505,15 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
     }
   g.m_low = 0;
   while (g.m_low < Cfg::TB && g.tile_pos[g.m_low] == g.m_low) ++g.m_low;
+  g.direct = 1;
+  for (int q = 0; q < 5; ++q)
+    if (g.tile_pos[q] != q || g.is_target[q]) g.direct = 0;
+  for (int c = 0; c < (1 << p.k); ++c) {
+    uint64_t d = 0;
+    for (int b = 0; b < p.k; ++b)
+      if ((c >> b) & 1) d |= uint64_t{1} << p.qubits[b];
+    g.cdep[c] = d;
+  }
   g.nh = 0;
   for (int i = g.m_low; i < Cfg::TB; ++i) g.hpos[g.nh++] = g.tile_pos[i];
   g.n_tiles = st.dim() >> Cfg::TB;
