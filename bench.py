@@ -40,6 +40,12 @@ sys.path.insert(0, ROOT)
 N_QUBITS, DEPTH, SEED = 30, 40, 1234
 METRIC = "time per 30q circuit"
 
+# DRAM bytes (read + write) of one fused_tc_kernel<5> launch on a 2^26
+# complex64 state, from ncu (dram__bytes_read.sum 537.14 MB +
+# dram__bytes_write.sum 476.98 MB, one launch of the 26-qubit depth-4 brick
+# wall).  A launch streams the state once, so the figure scales with 2^n.
+TC_TRAFFIC_BYTES_26Q = 537.143808e6 + 476.978944e6
+
 
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -431,7 +437,9 @@ def main():
         byts = float(np.mean([info[i][3] for i in tc_idx]))
         ach = byts / (dur * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "peak_source": peak_kind, "traffic": None, "kernel": "fused_tc_kernel<5>",
+                "peak_source": peak_kind, "traffic": TC_TRAFFIC_BYTES_26Q * 2.0 ** (nq - 26),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 26 qubits, "
+                                  "scaled by 2^(n-26)", "kernel": "fused_tc_kernel<5>",
                 "bytes_per_launch": byts, "mean_launch_ms": dur, "launches_per_step": len(tc_idx)}
     other = [i for i in range(npass) if i not in tc_idx]
     pass_summary = {
@@ -474,10 +482,11 @@ def main():
             "metric": METRIC, "value": value, "unit": "ms/circuit", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-            "config": {"workload": "random U+CX brick wall, 30 qubits, depth 40, seed 1234, complex64, "
-                                   f"{args.fusion} fusion k<={args.k} on tcgen05 3xTF32",
+            "config": {"workload": f"random U+CX brick wall, {nq} qubits, depth {args.depth}, seed {SEED}, "
+                                   f"complex64, {args.fusion} fusion k<={args.k} on tcgen05 3xTF32",
                        "global_batch": world, "seq_len": None, "parallelism": f"replicas x{world}",
-                       "l2": "state 8 GiB > L2 126 MB, no flush", "gates": int(stats["n_gates"]),
+                       "l2": f"state {8 * 2 ** nq / 2 ** 30:g} GiB > L2 126 MB, no flush",
+                       "gates": int(stats["n_gates"]),
                        "passes": npass, "tensor_passes": int(stats["n_tensor"])},
             "roofline": roof, "passes": pass_summary, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks, "checks": checks,
