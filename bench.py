@@ -269,9 +269,15 @@ def run_adjoint24(args):
             "value": batch * npar / t, "unit": "gradients/s", "higher_is_better": True,
             "seconds_per_batch": t, "batch": batch, "params": npar}
     if not args.no_checks:
+        t0 = time.perf_counter()
+        vpg, gpg = adjoint_expval(circ, pidx, theta, ham, "c64", 2, method="per_gate")
+        t_pg = time.perf_counter() - t0
         v128, g128 = adjoint_expval(circ, pidx, theta[:2], ham, "c128", 2)
         line["checks"] = {"max_abs_value_vs_fp64_adjoint": float(np.abs(vals[:2] - v128).max()),
-                          "max_abs_grad_vs_fp64_adjoint": float(np.abs(grads[:2] - g128).max())}
+                          "max_abs_grad_vs_fp64_adjoint": float(np.abs(grads[:2] - g128).max()),
+                          "per_gate_sweep_seconds_per_batch": t_pg,
+                          "per_gate_gradients_per_s": batch * npar / t_pg,
+                          "max_abs_grad_tiled_vs_per_gate": float(np.abs(grads - gpg).max())}
         # central finite differences (h = 1e-3) of the complex128 GPU forward
         h = 1e-3
         ks = np.random.default_rng(13).choice(npar, 6, replace=False)

@@ -205,6 +205,27 @@ int ketgpu_adjoint(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
                    const char* const* paulis, uint64_t n_terms,
                    int32_t precision, int32_t checkpoint_every, double* values,
                    double* grads);
+/* Sweep methods: AUTO = TILED when n_qubits >= the tile size (12 qubits
+ * for KETGPU_C64, 11 for KETGPU_C128), else PER_GATE.  PER_GATE streams the
+ * states through HBM once per gate; TILED runs each block of consecutive
+ * gates that fits one tile in shared memory and registers, one HBM pass per
+ * block.  Both give the same values and gradients up to rounding. */
+#define KETGPU_ADJOINT_AUTO 0
+#define KETGPU_ADJOINT_PER_GATE 1
+#define KETGPU_ADJOINT_TILED 2
+int ketgpu_adjoint_ex(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
+                      const int32_t* param_index, const double* params,
+                      uint64_t n_params, uint64_t batch, const double* coeffs,
+                      const char* const* paulis, uint64_t n_terms,
+                      int32_t precision, int32_t checkpoint_every,
+                      int32_t method, double* values, double* grads);
+/* The tiled sweeps' plan as flat int32 records (layout documented in
+ * ket_b200/csrc/adjoint.cu); *length receives the record count, out may be
+ * NULL to query it. */
+int ketgpu_adjoint_plan_describe(int32_t n_qubits, const ketgpu_op* ops,
+                                 uint64_t n_ops, const int32_t* param_index,
+                                 int32_t precision, int32_t* out,
+                                 uint64_t capacity, uint64_t* length);
 
 /* ---- learned fusion cost model (48 -> 128 -> 128 -> 1 MLP, BF16 weights,
  *      FP32 accumulation; no ket counterpart) ------------------------- */

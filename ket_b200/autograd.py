@@ -22,8 +22,11 @@ from .circuit import Circuit
 
 def adjoint_expval(circuit: Circuit, param_index: np.ndarray, params: np.ndarray,
                    hamiltonian: Sequence[Tuple[float, str]], precision: str = "c64",
-                   checkpoint_every: int = 2) -> Tuple[np.ndarray, np.ndarray]:
-    """values (batch,), grads (batch, n_params) for params of shape (batch, n_params)."""
+                   checkpoint_every: int = 2, method: str = "auto") -> Tuple[np.ndarray, np.ndarray]:
+    """values (batch,), grads (batch, n_params) for params of shape (batch, n_params).
+
+    method: "auto", "per_gate" or "tiled" (the sweep kernels; same results up
+    to rounding)."""
     ops = circuit.to_ops()
     pidx = np.ascontiguousarray(param_index, dtype=np.int32)
     if len(pidx) != len(ops):
@@ -35,9 +38,10 @@ def adjoint_expval(circuit: Circuit, param_index: np.ndarray, params: np.ndarray
     values = np.zeros(batch, dtype=np.float64)
     grads = np.zeros((batch, npar), dtype=np.float64)
     prec = {"c64": _lib.C64, "c128": _lib.C128}[precision]
-    check(lib.ketgpu_adjoint(circuit.n_qubits, ops.ctypes.data, len(ops), pidx.ctypes.data, prm.ctypes.data,
-                             npar, batch, coeffs.ctypes.data, ct.cast(arr, ct.c_void_p), len(hamiltonian),
-                             prec, int(checkpoint_every), values.ctypes.data, grads.ctypes.data))
+    meth = {"auto": 0, "per_gate": 1, "tiled": 2}[method]
+    check(lib.ketgpu_adjoint_ex(circuit.n_qubits, ops.ctypes.data, len(ops), pidx.ctypes.data, prm.ctypes.data,
+                                npar, batch, coeffs.ctypes.data, ct.cast(arr, ct.c_void_p), len(hamiltonian),
+                                prec, int(checkpoint_every), meth, values.ctypes.data, grads.ctypes.data))
     return values, grads
 
 

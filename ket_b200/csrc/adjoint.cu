@@ -23,6 +23,9 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <queue>
+#include <string>
+#include <utility>
 #include <vector>
 
 #include "internal.h"
@@ -242,6 +245,684 @@ __global__ void ground_batch(typename C2T<R>::T* states, uint64_t dim) {
   states[(uint64_t)blockIdx.x * dim] = one;
 }
 
+
+// ---------------------------------------------------------------------------
+// Tiled sweeps.  The per-gate kernels above stream psi (and lambda) through
+// HBM once per gate.  The tiled form groups consecutive gates into blocks
+// whose qubits fit one tile of TB qubits (always including qubits 0-4, so a
+// warp's 32 consecutive tile elements are 32 consecutive amplitudes), loads
+// each tile of psi and lambda into shared memory once, and runs the whole
+// block there: the forward applications, or in the reverse sweep the
+// gradient inner products and the inverse applications of every gate of the
+// block.  Inside a block, gates are run in phases: a phase names RB tile bits
+// that each thread holds in registers (2^RB amplitudes of each state), so
+// every gate whose target bits are among them is register arithmetic; a
+// diagonal gate needs no register bits at all.  Gradient partial sums are
+// formed per thread over its pairs in the state's precision, reduced across
+// the warp in FP64 and accumulated per warp and gate in shared memory (FP64),
+// then summed in fixed order over warps, CTAs and (on the host) blocks.
+
+template <typename R>
+struct TileCfg;
+template <>
+struct TileCfg<float> {
+  static constexpr int TB = 12, RB = 4;
+};
+template <>
+struct TileCfg<double> {
+  static constexpr int TB = 11, RB = 3;
+};
+constexpr int kTileThreads = 256;  // 2^(TB - RB) in both precisions
+constexpr int kTileWarps = kTileThreads / 32;
+constexpr int kMaxBlockGrads = 64;
+constexpr int kMaxBlockGates = 256;
+
+enum TKind : uint8_t { kTPair = 0, kTPairSwap = 1, kTSwap2 = 2, kTDiag = 3 };
+
+struct TGate {
+  uint8_t kind;
+  uint8_t s0, s1;  // register slots of the target(s) (pair kinds; s0 < s1 for kTSwap2)
+  int8_t tslot;    // kTDiag: register slot of the target bit, or -1
+  uint8_t tbit;    // kTDiag: tile bit of the target
+  uint8_t cm_r;    // controls held in registers, as a register-index mask
+  uint8_t gen;     // gradient generator: 0 none, 1 X, 2 Y, 3 Z, 4 P11
+  uint8_t real;    // kTPair: the matrix is real for every parameter set
+  uint16_t cm_g;   // controls not held in registers, as a tile-bit mask
+  int16_t grad;    // gradient slot within the block, or -1
+  int32_t mat;     // gate index into the per-set matrix table
+};
+static_assert(sizeof(TGate) == 16, "TGate layout");
+
+struct TPhase {
+  uint8_t r[4];  // tile bits held in registers (register-index bit b <-> r[b])
+  int32_t first, count;  // gates of the phase, relative to the block's first gate
+};
+
+struct TileGeom {
+  uint64_t n_tiles;
+  int pos[12];  // tile bit -> qubit, ascending; pos[0..4] = 0..4
+};
+
+// Shared-memory swizzle: XOR-folds the higher bit groups into the lowest so
+// that a half-warp (8-byte elements) or quarter-warp (16-byte elements)
+// touching 16 (8) elements that differ in any four (three) tile bits hits
+// distinct banks in the common layouts.
+template <typename R>
+__device__ __forceinline__ int tphys(int e);
+template <>
+__device__ __forceinline__ int tphys<float>(int e) {
+  return e ^ (((e >> 4) ^ (e >> 8)) & 15);
+}
+template <>
+__device__ __forceinline__ int tphys<double>(int e) {
+  return e ^ (((e >> 3) ^ (e >> 6) ^ (e >> 9)) & 7);
+}
+
+template <typename R>
+struct CM2 {
+  R r[4], i[4];
+};
+
+// m (U, row-major, 8 values re/im interleaved) or its conjugate transpose.
+template <typename R, bool DAG>
+__device__ __forceinline__ CM2<R> load_cm2(const R* m) {
+  CM2<R> c;
+  if (!DAG) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      c.r[k] = m[2 * k];
+      c.i[k] = m[2 * k + 1];
+    }
+  } else {
+    c.r[0] = m[0], c.i[0] = -m[1];
+    c.r[1] = m[4], c.i[1] = -m[5];
+    c.r[2] = m[2], c.i[2] = -m[3];
+    c.r[3] = m[6], c.i[3] = -m[7];
+  }
+  return c;
+}
+
+template <typename T, typename R>
+__device__ __forceinline__ void mul2(const CM2<R>& c, T& a, T& b) {
+  T x, y;
+  x.x = c.r[0] * a.x - c.i[0] * a.y + c.r[1] * b.x - c.i[1] * b.y;
+  x.y = c.r[0] * a.y + c.i[0] * a.x + c.r[1] * b.y + c.i[1] * b.x;
+  y.x = c.r[2] * a.x - c.i[2] * a.y + c.r[3] * b.x - c.i[3] * b.y;
+  y.y = c.r[2] * a.y + c.i[2] * a.x + c.r[3] * b.y + c.i[3] * b.x;
+  a = x;
+  b = y;
+}
+
+template <typename T, typename R>
+__device__ __forceinline__ void mul2_real(const CM2<R>& c, T& a, T& b) {
+  T x, y;
+  x.x = c.r[0] * a.x + c.r[1] * b.x;
+  x.y = c.r[0] * a.y + c.r[1] * b.y;
+  y.x = c.r[2] * a.x + c.r[3] * b.x;
+  y.y = c.r[2] * a.y + c.r[3] * b.y;
+  a = x;
+  b = y;
+}
+
+template <typename T, typename R>
+__device__ __forceinline__ void cmul(T& a, R pr, R pi) {
+  const R x = pr * a.x - pi * a.y;
+  a.y = pr * a.y + pi * a.x;
+  a.x = x;
+}
+
+template <typename T, typename R>
+__device__ __forceinline__ void tswap(T& a, T& b) {
+  const T t = a;
+  a = b;
+  b = t;
+}
+
+// Im <l|G|a> on one pair for the generators X (1), Y (2), Z (3).
+template <typename T, typename R>
+__device__ __forceinline__ R pair_grad(int gen, const T& a0, const T& a1, const T& l0, const T& l1) {
+  if (gen == 1) return (l0.x * a1.y - l0.y * a1.x) + (l1.x * a0.y - l1.y * a0.x);
+  if (gen == 2) return (l1.x * a0.x + l1.y * a0.y) - (l0.x * a1.x + l0.y * a1.y);
+  return (l0.x * a0.y - l0.y * a0.x) - (l1.x * a1.y - l1.y * a1.x);
+}
+
+// Gate bodies.  A thread holds the 2^RB register elements j of its group; S
+// (A, B) are register slots known at compile time; RC says whether some
+// control bits are register bits (then each j is tested against cm_r).
+// Forward (REV = false) applies U to p; reverse adds the gradient term and
+// applies U^dag to p and q.
+
+template <typename R, int RB, int S, bool REV, bool RC>
+__device__ __forceinline__ R tile_pair(typename C2T<R>::T* p, typename C2T<R>::T* q, const TGate& g,
+                                       const R* m) {
+  R part = 0;
+  if constexpr (S < RB) {
+    if (g.kind == kTPairSwap) {
+#pragma unroll
+      for (int j = 0; j < (1 << RB); ++j) {
+        if (j & (1 << S)) continue;
+        if (RC && (j & g.cm_r) != g.cm_r) continue;
+        tswap<typename C2T<R>::T, R>(p[j], p[j | (1 << S)]);
+        if (REV) tswap<typename C2T<R>::T, R>(q[j], q[j | (1 << S)]);
+      }
+      return part;
+    }
+    const CM2<R> c = load_cm2<R, REV>(m);
+    const bool real = g.real;
+    const int gen = REV ? g.gen : 0;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+      if (j & (1 << S)) continue;
+      const int j1 = j | (1 << S);
+      if (RC && (j & g.cm_r) != g.cm_r) continue;
+      if (REV && gen) part += pair_grad<typename C2T<R>::T, R>(gen, p[j], p[j1], q[j], q[j1]);
+      if (real) {
+        mul2_real(c, p[j], p[j1]);
+        if (REV) mul2_real(c, q[j], q[j1]);
+      } else {
+        mul2(c, p[j], p[j1]);
+        if (REV) mul2(c, q[j], q[j1]);
+      }
+    }
+  }
+  return part;
+}
+
+template <typename R, int RB, int A, int B, bool REV, bool RC>
+__device__ __forceinline__ void tile_swap2(typename C2T<R>::T* p, typename C2T<R>::T* q, const TGate& g) {
+  if constexpr (A < RB && B < RB && A < B) {
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+      if (!(j & (1 << A)) || (j & (1 << B))) continue;
+      if (RC && (j & g.cm_r) != g.cm_r) continue;
+      const int j1 = j ^ (1 << A) ^ (1 << B);
+      tswap<typename C2T<R>::T, R>(p[j], p[j1]);
+      if (REV) tswap<typename C2T<R>::T, R>(q[j], q[j1]);
+    }
+  }
+}
+
+// Diagonal gate whose target is register slot S: diag(m0, m3).
+template <typename R, int RB, int S, bool REV, bool RC>
+__device__ __forceinline__ R tile_diag_reg(typename C2T<R>::T* p, typename C2T<R>::T* q, const TGate& g,
+                                           const R* m) {
+  R part = 0;
+  if constexpr (S < RB) {
+    const R m0r = m[0], m0i = REV ? -m[1] : m[1], m3r = m[6], m3i = REV ? -m[7] : m[7];
+    const int gen = REV ? g.gen : 0;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+      if (RC && (j & g.cm_r) != g.cm_r) continue;
+      const bool bit = (j >> S) & 1;
+      if (REV && gen) {
+        const R im = q[j].x * p[j].y - q[j].y * p[j].x;  // Im(conj(l) a)
+        if (gen == 3) part += bit ? -im : im;
+        else if (bit) part += im;  // P11
+      }
+      cmul(p[j], bit ? m3r : m0r, bit ? m3i : m0i);
+      if (REV) cmul(q[j], bit ? m3r : m0r, bit ? m3i : m0i);
+    }
+  }
+  return part;
+}
+
+// Diagonal gate whose target is a group bit: one phase for all of the
+// thread's elements.
+template <typename R, int RB, bool REV, bool RC>
+__device__ __forceinline__ R tile_diag_grp(typename C2T<R>::T* p, typename C2T<R>::T* q, const TGate& g,
+                                           const R* m, bool bit) {
+  R part = 0;
+  const R pr = bit ? m[6] : m[0];
+  const R pi = REV ? -(bit ? m[7] : m[1]) : (bit ? m[7] : m[1]);
+  const int gen = REV ? g.gen : 0;
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if (RC && (j & g.cm_r) != g.cm_r) continue;
+    if (REV && gen) part += q[j].x * p[j].y - q[j].y * p[j].x;
+    cmul(p[j], pr, pi);
+    if (REV) cmul(q[j], pr, pi);
+  }
+  if (REV && gen) part = gen == 3 ? (bit ? -part : part) : (bit ? part : R(0));
+  return part;
+}
+
+template <typename R, int RB, bool REV, bool RC>
+__device__ __forceinline__ R tile_gate_rc(typename C2T<R>::T* p, typename C2T<R>::T* q, const TGate& g,
+                                          const R* m, int gbase) {
+  if (g.kind == kTDiag) {
+    switch (g.tslot) {
+      case 0: return tile_diag_reg<R, RB, 0, REV, RC>(p, q, g, m);
+      case 1: return tile_diag_reg<R, RB, 1, REV, RC>(p, q, g, m);
+      case 2: return tile_diag_reg<R, RB, 2, REV, RC>(p, q, g, m);
+      case 3: return tile_diag_reg<R, RB, 3, REV, RC>(p, q, g, m);
+      default: return tile_diag_grp<R, RB, REV, RC>(p, q, g, m, (gbase >> g.tbit) & 1);
+    }
+  }
+  if (g.kind == kTSwap2) {
+    switch (g.s0 * 4 + g.s1) {
+      case 1: tile_swap2<R, RB, 0, 1, REV, RC>(p, q, g); break;
+      case 2: tile_swap2<R, RB, 0, 2, REV, RC>(p, q, g); break;
+      case 3: tile_swap2<R, RB, 0, 3, REV, RC>(p, q, g); break;
+      case 6: tile_swap2<R, RB, 1, 2, REV, RC>(p, q, g); break;
+      case 7: tile_swap2<R, RB, 1, 3, REV, RC>(p, q, g); break;
+      case 11: tile_swap2<R, RB, 2, 3, REV, RC>(p, q, g); break;
+      default: break;
+    }
+    return 0;
+  }
+  switch (g.s0) {
+    case 0: return tile_pair<R, RB, 0, REV, RC>(p, q, g, m);
+    case 1: return tile_pair<R, RB, 1, REV, RC>(p, q, g, m);
+    case 2: return tile_pair<R, RB, 2, REV, RC>(p, q, g, m);
+    default: return tile_pair<R, RB, 3, REV, RC>(p, q, g, m);
+  }
+}
+
+template <typename R, int RB, bool REV>
+__device__ __forceinline__ R tile_gate(typename C2T<R>::T* p, typename C2T<R>::T* q, const TGate& g,
+                                       const R* m, int gbase) {
+  if ((gbase & g.cm_g) != g.cm_g) return 0;  // a group-bit control is 0 for this thread
+  return g.cm_r ? tile_gate_rc<R, RB, REV, true>(p, q, g, m, gbase)
+                : tile_gate_rc<R, RB, REV, false>(p, q, g, m, gbase);
+}
+
+// Asynchronous global -> shared copy of one amplitude (8 or 16 bytes).
+__device__ __forceinline__ void tile_cp_async(float2* dst, const float2* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void tile_cp_async(double2* dst, const double2* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Forward (REV = false: psi only, gates in order) or reverse (REV = true:
+// psi and lambda, gates in reverse order, gradient partials) over one block,
+// for every tile of every parameter set of the chunk (gridDim.y = set).  One
+// CTA per SM (the register arrays of both states need ~170 registers); the
+// next tile streams into a second buffer with cp.async while the current one
+// is processed.  Shared memory: two tile buffers (psi, then lambda in the
+// reverse), the block's gate records and this set's matrices, then the
+// per-warp gradient sums (reverse).
+template <typename R, bool REV>
+__global__ void __launch_bounds__(kTileThreads, 1)
+    tile_sweep(typename C2T<R>::T* __restrict__ psi, typename C2T<R>::T* __restrict__ lam, uint64_t dim,
+               TileGeom tg, const TGate* __restrict__ gates, int ngates, const TPhase* __restrict__ phases,
+               int nph, const R* __restrict__ mats, uint64_t mat_stride, int ngrad, double* __restrict__ partial) {
+  using T = typename C2T<R>::T;
+  constexpr int TB = TileCfg<R>::TB, RB = TileCfg<R>::RB, NR = 1 << RB, TILE = 1 << TB;
+  constexpr int BUF = (REV ? 2 : 1) * TILE;  // elements per buffer
+  extern __shared__ __align__(16) unsigned char tsm[];
+  T* bufs = reinterpret_cast<T*>(tsm);
+  TGate* sg = reinterpret_cast<TGate*>(tsm + 2 * BUF * sizeof(T));
+  R* smat = reinterpret_cast<R*>(sg + ngates);
+  double* acc = reinterpret_cast<double*>(smat + 8 * (size_t)ngates);  // [warp][ngrad]
+  __shared__ uint64_t off_lo[64], off_hi[64];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int set = blockIdx.y;
+  T* s = psi + (uint64_t)set * dim;
+  T* l = REV ? lam + (uint64_t)set * dim : nullptr;
+
+  if (tid < 128) {
+    const int half = tid >> 6, e = tid & 63;
+    uint64_t off = 0;
+    for (int b = 0; b < 6; ++b) {
+      const int tb = 6 * half + b;
+      if (tb < TB && ((e >> b) & 1)) off |= uint64_t{1} << tg.pos[tb];
+    }
+    (half ? off_hi : off_lo)[e] = off;
+  }
+  for (int i = tid; i < ngates; i += kTileThreads) {
+    const TGate g = gates[i];
+    sg[i] = g;
+    const R* src = mats + ((uint64_t)g.mat * mat_stride + set) * 8;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) smat[8 * i + k] = src[k];
+  }
+  if (REV)
+    for (int i = tid; i < kTileWarps * ngrad; i += kTileThreads) acc[i] = 0.0;
+  __syncthreads();
+
+  auto tile_base = [&](uint64_t t) {
+    uint64_t base = t;
+#pragma unroll
+    for (int b = 0; b < TB; ++b) {
+      const int f = tg.pos[b];
+      base = ((base >> f) << (f + 1)) | (base & ((uint64_t{1} << f) - 1));
+    }
+    return base;
+  };
+  auto prefetch = [&](uint64_t t, T* buf) {
+    const uint64_t base = tile_base(t);
+#pragma unroll 2
+    for (int r = 0; r < NR; ++r) {
+      const int e = tid + r * kTileThreads;
+      const uint64_t o = base + (off_lo[e & 63] | off_hi[e >> 6]);
+      tile_cp_async(buf + tphys<R>(e), s + o);
+      if (REV) tile_cp_async(buf + TILE + tphys<R>(e), l + o);
+    }
+  };
+
+  int cur = 0;
+  if (blockIdx.x < tg.n_tiles) prefetch(blockIdx.x, bufs);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  for (uint64_t t = blockIdx.x; t < tg.n_tiles; t += gridDim.x) {
+    T* sp = bufs + cur * BUF;
+    T* sl = sp + TILE;
+    if (t + gridDim.x < tg.n_tiles) prefetch(t + gridDim.x, bufs + (cur ^ 1) * BUF);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this tile's copies are done
+    __syncthreads();
+    for (int k = 0; k < nph; ++k) {
+      const TPhase P = phases[REV ? nph - 1 - k : k];
+      // group bits of this thread: the non-register tile bits, ascending
+      int rmask = 0;
+#pragma unroll
+      for (int b = 0; b < RB; ++b) rmask |= 1 << P.r[b];
+      int gbase = 0;
+      {
+        int kk = 0;
+#pragma unroll
+        for (int b = 0; b < TB; ++b)
+          if (!((rmask >> b) & 1)) {
+            gbase |= ((tid >> kk) & 1) << b;
+            ++kk;
+          }
+      }
+      // the swizzle is XOR-linear and gbase, rdep(j) have disjoint bits, so
+      // the address of element j is tphys(gbase) ^ tphys(rdep(j))
+      const int pg = tphys<R>(gbase);
+      int pb[RB];
+#pragma unroll
+      for (int b = 0; b < RB; ++b) pb[b] = tphys<R>(1 << P.r[b]);
+      T p[NR], q[NR];
+#pragma unroll
+      for (int j = 0; j < NR; ++j) {
+        int a = pg;
+#pragma unroll
+        for (int b = 0; b < RB; ++b)
+          if (j & (1 << b)) a ^= pb[b];
+        p[j] = sp[a];
+        if (REV) q[j] = sl[a];
+      }
+      for (int c = 0; c < P.count; ++c) {
+        const int gi = REV ? P.first + P.count - 1 - c : P.first + c;
+        const TGate g = sg[gi];
+        const R part = tile_gate<R, RB, REV>(p, q, g, smat + 8 * gi, gbase);
+        if (REV && g.grad >= 0) {
+          double v = (double)part;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) acc[warp * ngrad + g.grad] += v;
+        }
+      }
+      {
+        // element addresses again, from a fresh read of the phase record (so
+        // that the 2^RB addresses are not held in registers across the gates)
+        unsigned rw;
+        asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(rw) : "l"(&phases[REV ? nph - 1 - k : k]));
+        const int pg2 = tphys<R>(gbase);
+        int pb2[RB];
+#pragma unroll
+        for (int b = 0; b < RB; ++b) pb2[b] = tphys<R>(1 << ((rw >> (8 * b)) & 0xff));
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+          int a = pg2;
+#pragma unroll
+          for (int b = 0; b < RB; ++b)
+            if (j & (1 << b)) a ^= pb2[b];
+          sp[a] = p[j];
+          if (REV) sl[a] = q[j];
+        }
+      }
+      __syncthreads();
+    }
+    {
+      const uint64_t base = tile_base(t);
+      const volatile uint64_t* vlo = off_lo;
+      const volatile uint64_t* vhi = off_hi;
+#pragma unroll 2
+      for (int r = 0; r < NR; ++r) {
+        const int e = tid + r * kTileThreads;
+        const uint64_t o = base + (vlo[e & 63] | vhi[e >> 6]);
+        s[o] = sp[tphys<R>(e)];
+        if (REV) l[o] = sl[tphys<R>(e)];
+      }
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  if (REV)
+    for (int g = tid; g < ngrad; g += kTileThreads) {
+      double v = 0.0;
+      for (int w = 0; w < kTileWarps; ++w) v += acc[w * ngrad + g];
+      partial[((uint64_t)set * ngrad + g) * gridDim.x + blockIdx.x] = v;
+    }
+}
+
+// Host plan of the tiled sweeps.
+struct TBlock {
+  TileGeom geom;
+  int layer = 0;
+  int gate_first = 0, n_gates = 0;    // into the concatenated TGate array
+  int phase_first = 0, n_phases = 0;  // into the concatenated TPhase array
+  std::vector<int> grad_gate;         // gradient slot -> gate list index
+  size_t part_off = 0;                // into the gradient partials (doubles)
+};
+
+struct TilePlan {
+  std::vector<TBlock> blocks;
+  std::vector<TGate> gates;
+  std::vector<TPhase> phases;
+};
+
+// Target tile bits, controls and kind of a lowered gate, in tile bits.
+struct TileOp {
+  uint8_t kind;
+  int targets[2];
+  int ntargets;
+  int tgt_diag;  // kTDiag: target tile bit
+  int cmask;     // controls (tile bits)
+};
+
+TileOp tile_op_of(const Pass& p, const int* tpos_of_qubit) {
+  TileOp t{};
+  auto tile_mask = [&](uint64_t m) {
+    int r = 0;
+    for (int q = 0; q < 64; ++q)
+      if ((m >> q) & 1) r |= 1 << tpos_of_qubit[q];
+    return r;
+  };
+  if (p.kind == PassKind::Phase) {
+    // all fixed bits must be 1: the highest is the target, the rest controls
+    const int top = p.fixed[p.nfixed - 1];
+    t.kind = kTDiag;
+    t.tgt_diag = tpos_of_qubit[top];
+    t.cmask = tile_mask(p.p0 & ~(uint64_t{1} << top));
+    t.ntargets = 0;
+    return t;
+  }
+  const uint64_t diff = p.p0 ^ p.p1;
+  if (p.mode == kPairDiag) {
+    t.kind = kTDiag;
+    t.tgt_diag = tpos_of_qubit[__builtin_ctzll(diff)];
+    t.cmask = tile_mask(p.p0);
+    t.ntargets = 0;
+    return t;
+  }
+  if (__builtin_popcountll(diff) == 2) {
+    t.kind = kTSwap2;
+    const int a = __builtin_ctzll(diff), b = 63 - __builtin_clzll(diff);
+    t.targets[0] = tpos_of_qubit[a];
+    t.targets[1] = tpos_of_qubit[b];
+    t.ntargets = 2;
+    t.cmask = tile_mask(p.p0 & p.p1);
+    return t;
+  }
+  t.kind = p.mode == kPairSwap ? kTPairSwap : kTPair;
+  t.targets[0] = tpos_of_qubit[__builtin_ctzll(diff)];
+  t.ntargets = 1;
+  t.cmask = tile_mask(p.p0);
+  return t;
+}
+
+template <typename R>
+TilePlan plan_tiles(int n, const ketgpu_op* ops, const std::vector<int>& gate_ops, const std::vector<int>& layer_of,
+                    const std::vector<GateGeom>& geo, const std::vector<uint8_t>& real) {
+  constexpr int TB = TileCfg<R>::TB, RB = TileCfg<R>::RB;
+  TilePlan tp;
+  const int G = (int)gate_ops.size();
+  std::vector<uint64_t> qmask(G);
+  for (int i = 0; i < G; ++i) {
+    const ketgpu_op& o = ops[gate_ops[i]];
+    uint64_t m = 0;
+    for (int j = 0; j < gate_arity(o.type); ++j) m |= uint64_t{1} << o.q[j];
+    qmask[i] = m;
+  }
+  int i0 = 0;
+  while (i0 < G) {
+    int i1 = i0;
+    while (i1 < G && layer_of[i1] == layer_of[i0]) ++i1;
+    // A topological order of the layer that sweeps the qubits upwards: among
+    // the gates whose predecessors (earlier gates sharing a qubit) are
+    // placed, take the one with the lowest highest qubit.  Chains such as a
+    // CX ring then fall into consecutive tiles instead of being cut by the
+    // single-qubit gates listed before them.
+    std::vector<int> rem;
+    {
+      std::vector<std::vector<int>> on_qubit(n);
+      for (int i = i0; i < i1; ++i)
+        for (int q = 0; q < n; ++q)
+          if ((qmask[i] >> q) & 1) on_qubit[q].push_back(i);
+      std::vector<size_t> head(n, 0);
+      auto ready = [&](int i) {
+        for (int q = 0; q < n; ++q)
+          if (((qmask[i] >> q) & 1) && on_qubit[q][head[q]] != i) return false;
+        return true;
+      };
+      using Key = std::pair<int, int>;  // (highest qubit, original index)
+      std::priority_queue<Key, std::vector<Key>, std::greater<Key>> pq;
+      std::vector<uint8_t> queued(G, 0);
+      auto offer = [&](int i) {
+        if (!queued[i] && ready(i)) {
+          queued[i] = 1;
+          pq.push({63 - __builtin_clzll(qmask[i]), i});
+        }
+      };
+      for (int q = 0; q < n; ++q)
+        if (!on_qubit[q].empty()) offer(on_qubit[q][0]);
+      while (!pq.empty()) {
+        const int i = pq.top().second;
+        pq.pop();
+        rem.push_back(i);
+        for (int q = 0; q < n; ++q)
+          if ((qmask[i] >> q) & 1) {
+            ++head[q];
+            if (head[q] < on_qubit[q].size()) offer(on_qubit[q][head[q]]);
+          }
+      }
+    }
+    while (!rem.empty()) {
+      uint64_t S = 0x1f, blocked = 0;
+      std::vector<int> take, keep;
+      int ngrad = 0;
+      for (int i : rem) {
+        const bool grad = geo[i].gen && geo[i].pslot >= 0;
+        const uint64_t u = S | qmask[i];
+        if ((qmask[i] & blocked) || __builtin_popcountll(u) > TB || (int)take.size() >= kMaxBlockGates ||
+            (grad && ngrad >= kMaxBlockGrads)) {
+          blocked |= qmask[i];
+          keep.push_back(i);
+          continue;
+        }
+        S = u;
+        take.push_back(i);
+        ngrad += grad;
+      }
+      rem.swap(keep);
+      for (int q = 0; q < n && __builtin_popcountll(S) < TB; ++q) S |= uint64_t{1} << q;
+      TBlock b;
+      b.layer = layer_of[i0];
+      int tpos[64];
+      for (int q = 0, k = 0; q < n; ++q)
+        if ((S >> q) & 1) {
+          b.geom.pos[k] = q;
+          tpos[q] = k++;
+        }
+      for (int k = TB; k < 12; ++k) b.geom.pos[k] = 0;
+      b.geom.n_tiles = uint64_t{1} << (n - TB);
+      // phases: runs of gates whose target bits fit RB register bits
+      std::vector<TileOp> top(take.size());
+      for (size_t k = 0; k < take.size(); ++k) top[k] = tile_op_of(lower_gate(ops[gate_ops[take[k]]]), tpos);
+      b.gate_first = (int)tp.gates.size();
+      b.phase_first = (int)tp.phases.size();
+      size_t k0 = 0;
+      while (k0 < take.size()) {
+        int rmask = 0;
+        size_t k1 = k0;
+        for (; k1 < take.size(); ++k1) {
+          int need = 0;
+          for (int t = 0; t < top[k1].ntargets; ++t) need |= 1 << top[k1].targets[t];
+          if (__builtin_popcount(rmask | need) > RB) break;
+          rmask |= need;
+        }
+        for (int t = 0; t < TB && __builtin_popcount(rmask) < RB; ++t) rmask |= 1 << t;
+        TPhase ph{};
+        int slot_of[12];
+        for (int t = 0, k = 0; t < TB; ++t)
+          if ((rmask >> t) & 1) {
+            ph.r[k] = (uint8_t)t;
+            slot_of[t] = k++;
+          }
+        ph.first = (int)tp.gates.size() - b.gate_first;  // relative to the block's first gate
+        ph.count = (int)(k1 - k0);
+        for (size_t k = k0; k < k1; ++k) {
+          const TileOp& o = top[k];
+          const int gi = take[k];
+          TGate g{};
+          g.kind = o.kind;
+          g.mat = gi;
+          g.gen = geo[gi].pslot >= 0 ? (uint8_t)geo[gi].gen : 0;
+          g.real = real[gi];
+          g.tslot = -1;
+          int cm_r = 0, cm_g = 0;
+          for (int t = 0; t < TB; ++t)
+            if ((o.cmask >> t) & 1) {
+              if ((rmask >> t) & 1) cm_r |= 1 << slot_of[t];
+              else cm_g |= 1 << t;
+            }
+          g.cm_r = (uint8_t)cm_r;
+          g.cm_g = (uint16_t)cm_g;
+          if (o.kind == kTDiag) {
+            g.tbit = (uint8_t)o.tgt_diag;
+            if ((rmask >> o.tgt_diag) & 1) g.tslot = (int8_t)slot_of[o.tgt_diag];
+          } else if (o.kind == kTSwap2) {
+            const int a = slot_of[o.targets[0]], c = slot_of[o.targets[1]];
+            g.s0 = (uint8_t)std::min(a, c);
+            g.s1 = (uint8_t)std::max(a, c);
+          } else {
+            g.s0 = (uint8_t)slot_of[o.targets[0]];
+          }
+          g.grad = -1;
+          if (g.gen) {
+            g.grad = (int16_t)b.grad_gate.size();
+            b.grad_gate.push_back(gi);
+          }
+          tp.gates.push_back(g);
+        }
+        tp.phases.push_back(ph);
+        k0 = k1;
+      }
+      b.n_gates = (int)tp.gates.size() - b.gate_first;
+      b.n_phases = (int)tp.phases.size() - b.phase_first;
+      tp.blocks.push_back(std::move(b));
+    }
+    i0 = i1;
+  }
+  return tp;
+}
+
 struct DevBuf {
   void* p = nullptr;
   explicit DevBuf(size_t b) { KB_CUDA(cudaMalloc(&p, b ? b : 8)); }
@@ -268,10 +949,14 @@ template <typename R>
 void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx, const double* params,
                  uint64_t nparams, uint64_t batch, const std::vector<uint64_t>& flip,
                  const std::vector<uint64_t>& sign, const std::vector<int>& phq, const double* coeffs,
-                 int ckpt_every, double* values, double* grads) {
+                 int ckpt_every, int method, double* values, double* grads) {
   using T = typename C2T<R>::T;
+  constexpr int TB = TileCfg<R>::TB;
   const uint64_t dim = uint64_t{1} << n;
   const int T_ = (int)flip.size();
+  const bool tiled = method == KETGPU_ADJOINT_TILED || (method == KETGPU_ADJOINT_AUTO && n >= TB);
+  if (tiled && n < TB)
+    fail(KETGPU_ERR_INVALID, "adjoint: the tiled sweep needs at least " + std::to_string(TB) + " qubits");
   // gates (unitary ops) and layer boundaries (barriers)
   std::vector<int> gate_ops;
   std::vector<int> layer_of;
@@ -308,7 +993,6 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
   DevBuf psi(dim * sizeof(T) * chunk), lam(dim * sizeof(T) * chunk);
   DevBuf ck(dim * sizeof(T) * chunk * (size_t)n_ckpt);
   const int blocks = (int)std::min<uint64_t>(std::max<uint64_t>(1, (dim / 2 + kAThreads - 1) / kAThreads), 592);
-  DevBuf part(sizeof(double) * chunk * blocks * (G + 1));
   DevBuf mats(sizeof(double) * 8 * chunk * std::max<size_t>(G, 1));
   DevBuf hmeta(sizeof(uint64_t) * 2 * T_ + sizeof(int) * T_ + sizeof(double) * T_ + 64);
   {
@@ -343,26 +1027,82 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
     if (pi >= (int32_t)nparams) fail(KETGPU_ERR_OUT_OF_RANGE, "adjoint: parameter index out of range");
   }
 
+  // per-set 2x2 of gate gi (U, row-major, FP64 interleaved).  The tiled
+  // sweep stores a phase gate as diag(1, phase).
+  auto gate_matrix = [&](size_t gi, uint64_t set, double* d) {
+    ketgpu_op oo = ops[gate_ops[gi]];
+    if (geo[gi].pslot >= 0) oo.p[0] = params[set * nparams + geo[gi].pslot];
+    const Pass p = lower_gate(oo);
+    cplx mm[4] = {p.m[0], p.m[1], p.m[2], p.m[3]};
+    if (tiled && p.kind == PassKind::Phase) {
+      mm[3] = p.m[0];
+      mm[0] = cplx(1.0, 0.0);
+      mm[1] = mm[2] = cplx(0.0, 0.0);
+    }
+    for (int j = 0; j < 4; ++j) {
+      d[2 * j] = mm[j].real();
+      d[2 * j + 1] = mm[j].imag();
+    }
+  };
+
+  // tiled plan
+  TilePlan tp;
+  std::unique_ptr<DevBuf> d_tgates, d_tphases;
+  int gx = 1;
+  size_t grad_doubles = 0;
+  if (tiled) {
+    std::vector<uint8_t> real(G, 1);
+    double d[8];
+    for (size_t gi = 0; gi < G; ++gi)
+      for (uint64_t b = 0; b < batch && real[gi]; ++b) {
+        gate_matrix(gi, b, d);
+        if (d[1] != 0.0 || d[3] != 0.0 || d[5] != 0.0 || d[7] != 0.0) real[gi] = 0;
+        if (geo[gi].pslot < 0) break;  // the same matrix for every set
+      }
+    tp = plan_tiles<R>(n, ops, gate_ops, layer_of, geo, real);
+    d_tgates = std::make_unique<DevBuf>(sizeof(TGate) * std::max<size_t>(tp.gates.size(), 1));
+    d_tphases = std::make_unique<DevBuf>(sizeof(TPhase) * std::max<size_t>(tp.phases.size(), 1));
+    if (!tp.gates.empty())
+      KB_CUDA(cudaMemcpyAsync(d_tgates->p, tp.gates.data(), sizeof(TGate) * tp.gates.size(),
+                              cudaMemcpyHostToDevice, st));
+    if (!tp.phases.empty())
+      KB_CUDA(cudaMemcpyAsync(d_tphases->p, tp.phases.data(), sizeof(TPhase) * tp.phases.size(),
+                              cudaMemcpyHostToDevice, st));
+    const uint64_t n_tiles = uint64_t{1} << (n - TB);
+    // one CTA per SM: about 4 waves of 148 CTAs over the chunk's sets
+    gx = (int)std::min<uint64_t>(n_tiles, std::max<uint64_t>(1, (148ull * 4 + chunk - 1) / chunk));
+    for (TBlock& b : tp.blocks) {
+      b.part_off = grad_doubles;
+      grad_doubles += b.grad_gate.size() * chunk * (size_t)gx;
+    }
+    static bool attr_set[2] = {false, false};
+    if (!attr_set[sizeof(R) == 8]) {
+      const int per_gate = (int)(sizeof(TGate) + 8 * sizeof(R));
+      const int smem_rev = 4 * (1 << TB) * (int)sizeof(T) + kMaxBlockGates * per_gate + kTileWarps * kMaxBlockGrads * 8;
+      const int smem_fwd = 2 * (1 << TB) * (int)sizeof(T) + kMaxBlockGates * per_gate;
+      KB_CUDA(cudaFuncSetAttribute(tile_sweep<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rev));
+      KB_CUDA(cudaFuncSetAttribute(tile_sweep<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fwd));
+      attr_set[sizeof(R) == 8] = true;
+    }
+  }
+  const size_t ham_doubles = chunk * blocks;
+  DevBuf part(sizeof(double) * (tiled ? grad_doubles + ham_doubles : chunk * blocks * (G + 1)));
+  double* d_ham_part = part.as<double>() + (tiled ? grad_doubles : (size_t)G * chunk * blocks);
+
   std::vector<double> hmats(8 * chunk * std::max<size_t>(G, 1));
+  std::vector<R> hmats_t(tiled ? hmats.size() : 0);  // the tiled sweeps read them in the state's precision
+  DevBuf mats_t(sizeof(R) * std::max<size_t>(hmats_t.size(), 1));
   std::vector<double> hpart;
   for (uint64_t b0 = 0; b0 < batch; b0 += chunk) {
     const uint64_t nb = std::min(chunk, batch - b0);
-    // per-set matrices of every gate
-    for (size_t gi = 0; gi < G; ++gi) {
-      const ketgpu_op& o = ops[gate_ops[gi]];
-      for (uint64_t b = 0; b < nb; ++b) {
-        ketgpu_op oo = o;
-        if (geo[gi].pslot >= 0) oo.p[0] = params[(b0 + b) * nparams + geo[gi].pslot];
-        const Pass p = lower_gate(oo);
-        double* d = &hmats[(gi * chunk + b) * 8];
-        for (int j = 0; j < 4; ++j) {
-          d[2 * j] = p.m[j].real();
-          d[2 * j + 1] = p.m[j].imag();
-        }
-      }
-    }
+    for (size_t gi = 0; gi < G; ++gi)
+      for (uint64_t b = 0; b < nb; ++b) gate_matrix(gi, b0 + b, &hmats[(gi * chunk + b) * 8]);
     KB_CUDA(cudaMemcpyAsync(mats.p, hmats.data(), sizeof(double) * 8 * chunk * std::max<size_t>(G, 1),
                             cudaMemcpyHostToDevice, st));
+    if (tiled) {
+      for (size_t i = 0; i < hmats.size(); ++i) hmats_t[i] = (R)hmats[i];
+      KB_CUDA(cudaMemcpyAsync(mats_t.p, hmats_t.data(), sizeof(R) * hmats_t.size(), cudaMemcpyHostToDevice, st));
+    }
     // forward
     KB_CUDA(cudaMemsetAsync(psi.p, 0, dim * sizeof(T) * nb, st));
     ground_batch<R><<<(unsigned)nb, 1, 0, st>>>(psi.as<T>(), dim);
@@ -374,11 +1114,23 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
                               cudaMemcpyDeviceToDevice, st));
       ++next_ck;
     };
-    for (size_t gi = 0; gi < G; ++gi) {
-      while (next_ck < n_ckpt && next_ck * m <= layer_of[gi]) store_ck();
-      dim3 grid((unsigned)blocks, (unsigned)nb);
-      fwd_gate<R><<<grid, kAThreads, 0, st>>>(psi.as<T>(), dim, geo[gi], mats.as<double>() + gi * chunk * 8);
-      count_launch();
+    if (tiled) {
+      for (const TBlock& b : tp.blocks) {
+        while (next_ck < n_ckpt && next_ck * m <= b.layer) store_ck();
+        dim3 grid((unsigned)gx, (unsigned)nb);
+        const size_t smem = 2 * (size_t{1} << TB) * sizeof(T) + (size_t)b.n_gates * (sizeof(TGate) + 8 * sizeof(R));
+        tile_sweep<R, false><<<grid, kTileThreads, smem, st>>>(
+            psi.as<T>(), nullptr, dim, b.geom, d_tgates->as<TGate>() + b.gate_first, b.n_gates,
+            d_tphases->as<TPhase>() + b.phase_first, b.n_phases, mats_t.as<R>(), chunk, 0, nullptr);
+        count_launch();
+      }
+    } else {
+      for (size_t gi = 0; gi < G; ++gi) {
+        while (next_ck < n_ckpt && next_ck * m <= layer_of[gi]) store_ck();
+        dim3 grid((unsigned)blocks, (unsigned)nb);
+        fwd_gate<R><<<grid, kAThreads, 0, st>>>(psi.as<T>(), dim, geo[gi], mats.as<double>() + gi * chunk * 8);
+        count_launch();
+      }
     }
     while (next_ck < n_ckpt) store_ck();
     KB_CUDA(cudaGetLastError());
@@ -386,40 +1138,75 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
     {
       dim3 grid((unsigned)blocks, (unsigned)nb);
       ham_apply<R><<<grid, kAThreads, 0, st>>>(psi.as<T>(), lam.as<T>(), dim, d_flip, d_sign, d_q, d_coef, T_,
-                                               part.as<double>() + (size_t)G * chunk * blocks);
+                                               d_ham_part);
       count_launch();
     }
-    // reverse sweep; at the last gate of each segment (walking backwards)
-    // psi is reset to the checkpoint of the segment's end
-    for (size_t gi = G; gi-- > 0;) {
-      const int seg = layer_of[gi] / m;
-      if (gi + 1 < G && layer_of[gi + 1] / m != seg && seg + 1 < n_ckpt) {
-        KB_CUDA(cudaMemcpyAsync(psi.p, ck.as<T>() + (size_t)(seg + 1) * chunk * dim, dim * sizeof(T) * nb,
-                                cudaMemcpyDeviceToDevice, st));
+    // reverse sweep; at the last gate (block) of each segment, walking
+    // backwards, psi is reset to the checkpoint of the segment's end
+    if (tiled) {
+      const int B = (int)tp.blocks.size();
+      for (int bi = B; bi-- > 0;) {
+        const TBlock& b = tp.blocks[bi];
+        const int seg = b.layer / m;
+        if (bi + 1 < B && tp.blocks[bi + 1].layer / m != seg && seg + 1 < n_ckpt)
+          KB_CUDA(cudaMemcpyAsync(psi.p, ck.as<T>() + (size_t)(seg + 1) * chunk * dim, dim * sizeof(T) * nb,
+                                  cudaMemcpyDeviceToDevice, st));
+        const int ngrad = (int)b.grad_gate.size();
+        dim3 grid((unsigned)gx, (unsigned)nb);
+        const size_t smem = 4 * (size_t{1} << TB) * sizeof(T) +
+                            (size_t)b.n_gates * (sizeof(TGate) + 8 * sizeof(R)) + (size_t)kTileWarps * ngrad * 8;
+        tile_sweep<R, true><<<grid, kTileThreads, smem, st>>>(
+            psi.as<T>(), lam.as<T>(), dim, b.geom, d_tgates->as<TGate>() + b.gate_first, b.n_gates,
+            d_tphases->as<TPhase>() + b.phase_first, b.n_phases, mats_t.as<R>(), chunk, ngrad,
+            part.as<double>() + b.part_off);
+        count_launch();
       }
-      dim3 grid((unsigned)blocks, (unsigned)nb);
-      rev_gate<R><<<grid, kAThreads, 0, st>>>(psi.as<T>(), lam.as<T>(), dim, geo[gi],
-                                              mats.as<double>() + gi * chunk * 8,
-                                              part.as<double>() + gi * chunk * blocks);
-      count_launch();
+    } else {
+      for (size_t gi = G; gi-- > 0;) {
+        const int seg = layer_of[gi] / m;
+        if (gi + 1 < G && layer_of[gi + 1] / m != seg && seg + 1 < n_ckpt) {
+          KB_CUDA(cudaMemcpyAsync(psi.p, ck.as<T>() + (size_t)(seg + 1) * chunk * dim, dim * sizeof(T) * nb,
+                                  cudaMemcpyDeviceToDevice, st));
+        }
+        dim3 grid((unsigned)blocks, (unsigned)nb);
+        rev_gate<R><<<grid, kAThreads, 0, st>>>(psi.as<T>(), lam.as<T>(), dim, geo[gi],
+                                                mats.as<double>() + gi * chunk * 8,
+                                                part.as<double>() + gi * chunk * blocks);
+        count_launch();
+      }
     }
     KB_CUDA(cudaGetLastError());
-    hpart.resize((G + 1) * chunk * blocks);
-    KB_CUDA(cudaMemcpyAsync(hpart.data(), part.p, sizeof(double) * hpart.size(), cudaMemcpyDeviceToHost, st));
+    const size_t part_count = tiled ? grad_doubles + ham_doubles : (G + 1) * chunk * blocks;
+    hpart.resize(part_count);
+    KB_CUDA(cudaMemcpyAsync(hpart.data(), part.p, sizeof(double) * part_count, cudaMemcpyDeviceToHost, st));
     KB_CUDA(cudaStreamSynchronize(st));
+    const double* hham = hpart.data() + (tiled ? grad_doubles : (size_t)G * chunk * blocks);
     for (uint64_t b = 0; b < nb; ++b) {
       double v = 0;
-      const double* pv = &hpart[(size_t)G * chunk * blocks + b * blocks];
+      const double* pv = hham + b * blocks;
       for (int k = 0; k < blocks; ++k) v += pv[k];
       values[b0 + b] = v;
       double* gr = grads + (b0 + b) * nparams;
       for (uint64_t k = 0; k < nparams; ++k) gr[k] = 0.0;
-      for (size_t gi = 0; gi < G; ++gi) {
-        if (geo[gi].pslot < 0) continue;
-        double acc = 0;
-        const double* pg = &hpart[gi * chunk * blocks + b * blocks];
-        for (int k = 0; k < blocks; ++k) acc += pg[k];
-        gr[geo[gi].pslot] += (geo[gi].gen == 4) ? -2.0 * acc : acc;
+      if (tiled) {
+        for (const TBlock& blk : tp.blocks) {
+          const size_t ng = blk.grad_gate.size();
+          for (size_t k = 0; k < ng; ++k) {
+            const size_t gi = (size_t)blk.grad_gate[k];
+            const double* pg = &hpart[blk.part_off + (b * ng + k) * gx];
+            double acc = 0;
+            for (int c = 0; c < gx; ++c) acc += pg[c];
+            gr[geo[gi].pslot] += (geo[gi].gen == 4) ? -2.0 * acc : acc;
+          }
+        }
+      } else {
+        for (size_t gi = 0; gi < G; ++gi) {
+          if (geo[gi].pslot < 0) continue;
+          double acc = 0;
+          const double* pg = &hpart[gi * chunk * blocks + b * blocks];
+          for (int k = 0; k < blocks; ++k) acc += pg[k];
+          gr[geo[gi].pslot] += (geo[gi].gen == 4) ? -2.0 * acc : acc;
+        }
       }
     }
   }
@@ -430,26 +1217,118 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
 
 using namespace kb;
 
-KB_API int ketgpu_adjoint(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const int32_t* param_index,
-                          const double* params, uint64_t n_params, uint64_t batch, const double* coeffs,
-                          const char* const* paulis, uint64_t n_terms, int32_t precision, int32_t checkpoint_every,
-                          double* values, double* grads) {
+namespace {
+int adjoint_entry(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const int32_t* param_index, const double* params,
+                  uint64_t n_params, uint64_t batch, const double* coeffs, const char* const* paulis,
+                  uint64_t n_terms, int32_t precision, int32_t checkpoint_every, int32_t method, double* values,
+                  double* grads) {
   try {
     if (n < 1 || n > 34) fail(KETGPU_ERR_INVALID, "adjoint: n_qubits must be in [1, 34]");
     if (!ops || !values || !grads || (n_params && !params) || !coeffs || !paulis || n_terms == 0)
       fail(KETGPU_ERR_INVALID, "adjoint: null argument");
+    if (method < KETGPU_ADJOINT_AUTO || method > KETGPU_ADJOINT_TILED) fail(KETGPU_ERR_INVALID, "adjoint: bad method");
     validate_ops(n, ops, n_ops);
     std::vector<uint64_t> flip(n_terms), sign(n_terms);
     std::vector<int> q(n_terms);
     for (uint64_t t = 0; t < n_terms; ++t) pauli_masks(n, paulis[t], flip[t], sign[t], q[t]);
     if (precision == KETGPU_C64)
       run_adjoint<float>(n, ops, n_ops, param_index, params, n_params, batch, flip, sign, q, coeffs,
-                         checkpoint_every, values, grads);
+                         checkpoint_every, method, values, grads);
     else if (precision == KETGPU_C128)
       run_adjoint<double>(n, ops, n_ops, param_index, params, n_params, batch, flip, sign, q, coeffs,
-                          checkpoint_every, values, grads);
+                          checkpoint_every, method, values, grads);
     else
       fail(KETGPU_ERR_INVALID, "adjoint: bad precision");
+    return KETGPU_OK;
+  } catch (const Error& e) {
+    kb::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    kb::set_last_error(e.what());
+    return KETGPU_ERR_LOGIC;
+  }
+}
+}  // namespace
+
+KB_API int ketgpu_adjoint(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const int32_t* param_index,
+                          const double* params, uint64_t n_params, uint64_t batch, const double* coeffs,
+                          const char* const* paulis, uint64_t n_terms, int32_t precision, int32_t checkpoint_every,
+                          double* values, double* grads) {
+  return adjoint_entry(n, ops, n_ops, param_index, params, n_params, batch, coeffs, paulis, n_terms, precision,
+                       checkpoint_every, KETGPU_ADJOINT_AUTO, values, grads);
+}
+
+KB_API int ketgpu_adjoint_ex(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const int32_t* param_index,
+                             const double* params, uint64_t n_params, uint64_t batch, const double* coeffs,
+                             const char* const* paulis, uint64_t n_terms, int32_t precision,
+                             int32_t checkpoint_every, int32_t method, double* values, double* grads) {
+  return adjoint_entry(n, ops, n_ops, param_index, params, n_params, batch, coeffs, paulis, n_terms, precision,
+                       checkpoint_every, method, values, grads);
+}
+
+// Plan of the tiled sweeps as flat int32 records, for inspection and for
+// checking the plan on the host: [n_blocks] then per block
+// [layer, pos[12], n_phases, n_gates, phases (r0 r1 r2 r3 first count) ...,
+//  gates (kind s0 s1 tslot tbit cm_r cm_g gen real grad op_index) ...],
+// phase.first relative to the block's first gate.  Angles are taken from
+// the ops as given (the real flag is per those angles).
+KB_API int ketgpu_adjoint_plan_describe(int32_t n, const ketgpu_op* ops, uint64_t n_ops,
+                                        const int32_t* param_index, int32_t precision, int32_t* out,
+                                        uint64_t capacity, uint64_t* length) {
+  try {
+    if (!ops || !length) fail(KETGPU_ERR_INVALID, "adjoint_plan_describe: null argument");
+    validate_ops(n, ops, n_ops);
+    const int TB = precision == KETGPU_C64 ? TileCfg<float>::TB : TileCfg<double>::TB;
+    if (n < TB) fail(KETGPU_ERR_INVALID, "adjoint_plan_describe: fewer qubits than a tile");
+    std::vector<int> gate_ops, layer_of;
+    int layer = 0;
+    for (uint64_t i = 0; i < n_ops; ++i) {
+      if (ops[i].type == KETGPU_BARRIER) {
+        ++layer;
+        continue;
+      }
+      if (!is_unitary(ops[i].type)) continue;
+      gate_ops.push_back((int)i);
+      layer_of.push_back(layer);
+    }
+    std::vector<GateGeom> geo(gate_ops.size());
+    std::vector<uint8_t> real(gate_ops.size(), 0);
+    for (size_t gi = 0; gi < gate_ops.size(); ++gi) {
+      const ketgpu_op& o = ops[gate_ops[gi]];
+      const int32_t pi = param_index ? param_index[gate_ops[gi]] : -1;
+      geo[gi].pslot = pi;
+      geo[gi].gen = pi >= 0 ? gen_of(o.type) : 0;
+      const Pass p = lower_gate(o);
+      bool r = true;
+      for (int j = 0; j < 4; ++j) r = r && p.m[j].imag() == 0.0;
+      real[gi] = r && p.kind == PassKind::Pair;
+    }
+    const TilePlan tp = precision == KETGPU_C64 ? plan_tiles<float>(n, ops, gate_ops, layer_of, geo, real)
+                                                : plan_tiles<double>(n, ops, gate_ops, layer_of, geo, real);
+    std::vector<int32_t> v;
+    v.push_back((int32_t)tp.blocks.size());
+    for (const TBlock& b : tp.blocks) {
+      v.push_back(b.layer);
+      for (int k = 0; k < 12; ++k) v.push_back(b.geom.pos[k]);
+      v.push_back(b.n_phases);
+      v.push_back(b.n_gates);
+      for (int k = 0; k < b.n_phases; ++k) {
+        const TPhase& ph = tp.phases[b.phase_first + k];
+        for (int j = 0; j < 4; ++j) v.push_back(ph.r[j]);
+        v.push_back(ph.first);
+        v.push_back(ph.count);
+      }
+      for (int k = 0; k < b.n_gates; ++k) {
+        const TGate& g = tp.gates[b.gate_first + k];
+        v.insert(v.end(), {g.kind, g.s0, g.s1, g.tslot, g.tbit, g.cm_r, g.cm_g, g.gen, g.real, g.grad,
+                           gate_ops[g.mat]});
+      }
+    }
+    *length = v.size();
+    if (out) {
+      if (capacity < v.size()) fail(KETGPU_ERR_INVALID, "adjoint_plan_describe: buffer too small");
+      std::memcpy(out, v.data(), v.size() * sizeof(int32_t));
+    }
     return KETGPU_OK;
   } catch (const Error& e) {
     kb::set_last_error(e.what());

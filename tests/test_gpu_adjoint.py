@@ -137,3 +137,80 @@ def test_adjoint_errors():
     c2.ry(0, 0.0)
     with pytest.raises(ValueError):  # bad Pauli string
         adjoint_expval(c2, np.array([0], dtype=np.int32), np.zeros((1, 1)), [(1.0, "ZZ")], "c128")
+
+
+def _mixed_circuit(n, count, seed, barriers=3):
+    """Every gate kind ket has, with barriers; the rotations are parameters."""
+    from oracle.oracle import ARITY, GATES, NPARAMS, make_ops
+    rng = np.random.default_rng(seed)
+    gs, pidx = [], []
+    k = 0
+    pool = [g for g in GATES if ARITY[g] >= 1]
+    step = count // barriers + 1
+    for i in range(count):
+        if barriers and i % step == step - 1:
+            gs.append(("Barrier", []))
+            pidx.append(-1)
+            continue
+        g = pool[int(rng.integers(len(pool)))]
+        qs = [int(x) for x in rng.choice(n, ARITY[g], replace=False)]
+        ps = [float(x) for x in rng.uniform(0, 2 * math.pi, NPARAMS.get(g, 0))]
+        gs.append((g, qs, ps))
+        pidx.append(k if g in ("Rx", "Ry", "Rz", "CRx", "CRy", "CRz", "CP") else -1)
+        k += pidx[-1] >= 0
+    return make_ops(gs), np.array(pidx, dtype=np.int32), k
+
+
+class _OpsCircuit:
+    """Minimal circuit wrapper for adjoint_expval over a raw op array."""
+
+    def __init__(self, n, ops):
+        self.n_qubits = n
+        self._ops = ops
+
+    def to_ops(self):
+        return self._ops
+
+
+@pytest.mark.parametrize("prec,n,tol", [("c128", 11, 1e-9), ("c128", 13, 1e-9), ("c64", 12, 1e-5),
+                                        ("c64", 14, 1e-5)])
+@pytest.mark.parametrize("ckpt", [0, 1])
+def test_tiled_sweep_matches_fp64_oracle(oracle, prec, n, tol, ckpt):
+    """The tiled sweeps (blocks of gates in shared memory) against the FP64
+    oracle adjoint, over every gate kind, with barriers and checkpoints."""
+    from ket_b200.autograd import adjoint_expval
+    from ket_b200.workloads import random_pauli_sum
+    ops, pidx, npar = _mixed_circuit(n, 120, seed=n + 7 * ckpt)
+    circ = _OpsCircuit(n, ops)
+    ham = random_pauli_sum(n, 10, seed=n)
+    thetas = np.random.default_rng(n + 1).uniform(-math.pi, math.pi, (3, npar))
+    vals, grads = adjoint_expval(circ, pidx, thetas, ham, prec, checkpoint_every=ckpt, method="tiled")
+    for b in range(3):
+        v, g = oracle.adjoint(n, ops, pidx, thetas[b], ham)
+        assert abs(vals[b] - v) < tol
+        assert np.abs(grads[b] - g).max() < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("c128", 1e-10), ("c64", 2e-5)])
+def test_tiled_and_per_gate_sweeps_agree(prec, tol):
+    """The 24-qubit ansatz shape at 15 qubits: both sweep methods."""
+    from ket_b200.autograd import adjoint_expval
+    from ket_b200.workloads import random_pauli_sum, variational_ansatz
+    n = 15
+    circ, pidx = variational_ansatz(n, 6)
+    npar = int((pidx >= 0).sum())
+    ham = random_pauli_sum(n, 32, seed=21)
+    theta = np.random.default_rng(22).uniform(-math.pi, math.pi, (5, npar))
+    v1, g1 = adjoint_expval(circ, pidx, theta, ham, prec, checkpoint_every=2, method="per_gate")
+    v2, g2 = adjoint_expval(circ, pidx, theta, ham, prec, checkpoint_every=2, method="tiled")
+    assert np.abs(v1 - v2).max() < tol
+    assert np.abs(g1 - g2).max() < tol
+
+
+def test_tiled_sweep_needs_a_full_tile():
+    from ket_b200.autograd import adjoint_expval
+    from ket_b200.workloads import variational_ansatz
+    circ, pidx = variational_ansatz(10, 1)
+    npar = int((pidx >= 0).sum())
+    with pytest.raises(ValueError):
+        adjoint_expval(circ, pidx, np.zeros((1, npar)), [(1.0, "Z" * 10)], "c64", method="tiled")
