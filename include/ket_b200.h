@@ -133,8 +133,9 @@ int ketgpu_plan_execute(const ketgpu_plan* p, ketgpu_state* s);
 /* Execute and time every pass with CUDA events on the state's stream;
  * pass_ms receives n_passes durations (milliseconds).  Synchronises. */
 int ketgpu_plan_execute_timed(const ketgpu_plan* p, ketgpu_state* s, float* pass_ms);
-/* Describe pass `index`: kind (0 pair, 1 phase, 2 dense block), block
- * qubits k, tensor-core flag and algorithmic HBM bytes. */
+/* Describe pass `index`: kind (0 pair, 1 phase, 2 dense block, 3 norm
+ * capture/restore, 4 diagonal run), qubits k (block qubits, or the qubits a
+ * diagonal run touches), tensor-core flag and algorithmic HBM bytes. */
 int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* kind, int32_t* k,
                           int32_t* tensor, double* bytes);
 /* The state's CUDA stream (a cudaStream_t), for callers that order their

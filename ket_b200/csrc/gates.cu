@@ -452,7 +452,7 @@ void launch_fused_simt(const State& st, const Pass& p, const void* mat_t) {
 
 double Pass::bytes(int n, size_t amp) const {
   const double dim = (double)(uint64_t{1} << n);
-  if (kind == PassKind::Fused) return 2.0 * amp * dim;
+  if (kind == PassKind::Fused || kind == PassKind::Diagonal) return 2.0 * amp * dim;
   if (kind == PassKind::NormCapture) return amp * dim;
   if (kind == PassKind::NormRestore) return 3.0 * amp * dim;
   if (kind == PassKind::Phase) return 2.0 * amp * dim / (double)(uint64_t{1} << nfixed);
@@ -478,6 +478,10 @@ void launch_pass(const State& s, const Plan& plan, const Pass& p) {
   if (p.kind == PassKind::NormRestore) {
     norm_to_device(s, plan.d_norm + 2, plan.d_norm + 1);
     rescale_state(s, plan.d_norm, plan.d_norm + 1);
+    return;
+  }
+  if (p.kind == PassKind::Diagonal) {
+    launch_diag(s, p, static_cast<const char*>(plan.d_diag) + plan.offdiag[p.diag_index]);
     return;
   }
   if (p.kind != PassKind::Fused) {

@@ -58,6 +58,8 @@ enum class PassKind : int {
   Fused,     // dense 2^k x 2^k complex matrix on k qubits
   NormCapture,  // record the state's squared norm (FP64) on the device
   NormRestore,  // rescale the state to the recorded squared norm
+  Diagonal,     // multiply amplitude x by exp(i phi(x)), phi a quadratic
+                // polynomial in the index bits (a run of diagonal gates)
 };
 enum PairMode : int { kPairGeneral = 0, kPairSwap = 1, kPairDiag = 2 };
 
@@ -73,10 +75,22 @@ struct Pass {
   int qubits[6] = {0, 0, 0, 0, 0, 0};  // sorted ascending; matrix bit b <-> qubits[b]
   size_t mat_index = 0;                // into Plan::matrices
   bool tensor = false;                 // tcgen05 path
+  size_t diag_index = 0;               // Diagonal: into Plan::diags
   int first_op = 0, n_gates = 0;       // provenance
   std::vector<int> gates;              // op indices of the gates this pass applies
   double bytes(int n, size_t amp) const;
 };
+
+// Phase polynomial of a run of diagonal gates: the amplitude with index bits
+// x_0..x_{n-1} is multiplied by exp(i phi(x)),
+//   phi(x) = c0 + sum_i a[i] x_i + sum_{i<j} b[i*n + j] x_i x_j.
+struct DiagPoly {
+  double c0 = 0.0;
+  std::vector<double> a;  // n
+  std::vector<double> b;  // n x n, upper triangle used
+};
+// Low index bits whose pair terms are tabulated by the diagonal kernel.
+constexpr int kDiagLowBits = 12;
 
 struct Plan {
   int n = 0;
@@ -90,7 +104,9 @@ struct Plan {
   void* d_mat32 = nullptr;
   void* d_tc = nullptr;
   double* d_norm = nullptr;  // [captured, current, block partials...]
-  std::vector<size_t> off64, off32, offtc;
+  std::vector<DiagPoly> diags;  // Diagonal passes (host)
+  void* d_diag = nullptr;       // per Diagonal pass: low-bit table + coefficients
+  std::vector<size_t> off64, off32, offtc, offdiag;
   int device = -1;
   ketgpu_plan_stats stats{};
   ~Plan();
@@ -137,6 +153,13 @@ void learned_predict(const std::vector<float>& rows, std::vector<float>& us);
 void launch_pass(const State& s, const Plan& plan, const Pass& p);
 void upload_plan_matrices(Plan& plan, int device);
 void launch_fused_tc(const State& s, const Pass& p, const void* b_image);
+// Diagonal pass: device data = table (2^L complex, state precision) then FP64
+// coefficients, laid out by diag_device_data (diag.cu).
+void launch_diag(const State& s, const Pass& p, const void* data);
+void diag_device_data(const DiagPoly& poly, int n, int precision, std::vector<unsigned char>& out);
+bool is_diagonal_gate(int type);
+// Add one diagonal gate's phase terms to a polynomial.
+void add_diagonal_gate(const ketgpu_op& op, DiagPoly& poly, int n);
 // Size in bytes of one tcgen05 B image for a k-qubit block.
 size_t tc_image_bytes(int k);
 void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& out);

@@ -239,7 +239,14 @@ namespace {
 struct Block {
   std::vector<int> gates;  // op indices, program order
   std::vector<int> qubits; // sorted
+  bool diag = false;       // a run of diagonal gates: one Diagonal pass
 };
+
+uint64_t qubit_mask(const ketgpu_op& o) {
+  uint64_t m = 0;
+  for (int j = 0; j < gate_arity(o.type); ++j) m |= uint64_t{1} << o.q[j];
+  return m;
+}
 
 // Cost (in full-state passes) of a dense k-qubit block pass: one HBM pass,
 // plus the compute that outgrows it at large k.
@@ -253,15 +260,48 @@ bool block_on_tensor_cores(int n, int k, const PlanOptions& opt) {
   return opt.precision == KETGPU_C64 && opt.tensor && tc_supported(k) && n >= k + 7;
 }
 
-// Greedy DAG-aware block growth over the gates `order` of `ops`.
-std::vector<Block> grow_blocks(int n, const ketgpu_op* ops, const std::vector<int>& order, int max_k) {
+// Greedy DAG-aware block growth over the gates `order` of `ops`.  With
+// diag_runs, whenever the next gate to place is diagonal, every diagonal gate
+// that can be moved to the front of what is left (no earlier non-diagonal
+// gate shares a qubit with it) is collected; if that run spans more qubits
+// than one block holds, it becomes a single Diagonal pass.
+std::vector<Block> grow_blocks(int n, const ketgpu_op* ops, const std::vector<int>& order, int max_k,
+                               bool diag_runs) {
   std::vector<Block> blocks;
   std::vector<char> done(order.size(), 0);
   size_t first = 0;
   std::vector<char> blocked(n, 0), inq(n, 0);
+  const uint64_t all = n >= 64 ? ~uint64_t{0} : ((uint64_t{1} << n) - 1);
   while (true) {
     while (first < order.size() && done[first]) ++first;
     if (first == order.size()) break;
+    if (diag_runs && is_diagonal_gate(ops[order[first]].type)) {
+      std::vector<size_t> run;
+      uint64_t blk = 0, span = 0;
+      for (size_t i = first; i < order.size() && blk != all; ++i) {
+        if (done[i]) continue;
+        const ketgpu_op& o = ops[order[i]];
+        const uint64_t m = qubit_mask(o);
+        if (is_diagonal_gate(o.type) && !(m & blk)) {
+          run.push_back(i);
+          span |= m;
+        } else {
+          blk |= m;
+        }
+      }
+      if (run.size() >= 2 && __builtin_popcountll(span) > max_k) {
+        Block b;
+        b.diag = true;
+        for (size_t i : run) {
+          done[i] = 1;
+          b.gates.push_back(order[i]);
+        }
+        for (int q = 0; q < n; ++q)
+          if ((span >> q) & 1) b.qubits.push_back(q);
+        blocks.push_back(std::move(b));
+        continue;
+      }
+    }
     Block b;
     std::fill(blocked.begin(), blocked.end(), 0);
     std::fill(inq.begin(), inq.end(), 0);
@@ -339,6 +379,22 @@ void emit_single(Plan& plan, const ketgpu_op& o, int idx) {
   p.first_op = idx;
   p.n_gates = 1;
   p.gates = {idx};
+  plan.passes.push_back(p);
+}
+
+void emit_diagonal(Plan& plan, int n, const ketgpu_op* ops, const Block& b) {
+  DiagPoly poly;
+  poly.a.assign(n, 0.0);
+  poly.b.assign((size_t)n * n, 0.0);
+  for (int gi : b.gates) add_diagonal_gate(ops[gi], poly, n);
+  Pass p;
+  p.kind = PassKind::Diagonal;
+  p.k = (int)b.qubits.size();
+  p.diag_index = plan.diags.size();
+  p.first_op = b.gates.front();
+  p.n_gates = (int)b.gates.size();
+  p.gates = b.gates;
+  plan.diags.push_back(std::move(poly));
   plan.passes.push_back(p);
 }
 
@@ -466,7 +522,7 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
       // block taking its cheaper form.
       const int kmax_cap = std::max(2, std::min(6, opt.max_k + 1));
       std::vector<std::vector<Block>> cands;
-      for (int kc = 3; kc <= kmax_cap; ++kc) cands.push_back(grow_blocks(n, ops, seg, kc));
+      for (int kc = 3; kc <= kmax_cap; ++kc) cands.push_back(grow_blocks(n, ops, seg, kc, true));
       std::vector<float> rows;
       float fr[kFeatures];
       // single-gate rows, one per gate of the segment
@@ -480,6 +536,10 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
       std::vector<std::vector<size_t>> fused_row(cands.size());
       for (size_t c = 0; c < cands.size(); ++c)
         for (const Block& b : cands[c]) {
+          if (b.diag) {  // a Diagonal pass: scored as one full-state pass of its gates
+            fused_row[c].push_back(0);
+            continue;
+          }
           std::vector<const ketgpu_op*> gs;
           for (int gi : b.gates) gs.push_back(&ops[gi]);
           pass_features(n, opt.precision, gs, b.qubits, true,
@@ -496,6 +556,10 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
         double tot = 0;
         for (size_t bi = 0; bi < cands[c].size(); ++bi) {
           const Block& b = cands[c][bi];
+          if (b.diag) {
+            choice[c].push_back(2);
+            continue;
+          }
           double sep = 0;
           for (int gi : b.gates) sep += us[single_row[gi]];
           const double fu = us[fused_row[c][bi]];
@@ -511,12 +575,17 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
       predicted += best_t;
       for (size_t bi = 0; bi < cands[best].size(); ++bi) {
         const Block& b = cands[best][bi];
-        if (choice[best][bi]) emit_fused(plan, n, ops, b, opt);
+        if (choice[best][bi] == 2) emit_diagonal(plan, n, ops, b);
+        else if (choice[best][bi]) emit_fused(plan, n, ops, b, opt);
         else
           for (int gi : b.gates) emit_single(plan, ops[gi], gi);
       }
     } else {
-      for (const Block& b : grow_blocks(n, ops, seg, std::max(1, opt.max_k))) {
+      for (const Block& b : grow_blocks(n, ops, seg, std::max(1, opt.max_k), true)) {
+        if (b.diag) {
+          emit_diagonal(plan, n, ops, b);
+          continue;
+        }
         if (b.gates.size() == 1) {
           emit_single(plan, ops[b.gates[0]], b.gates[0]);
           continue;

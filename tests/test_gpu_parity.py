@@ -211,3 +211,56 @@ def test_uniform_stream_is_std_mt19937(golden):
         assert np.array_equal(kb.uniforms(seed, 2000), m[f"uniforms_{seed}"])
     r = MT19937(42)
     assert [r.canonical() for _ in range(5)] == list(m["uniforms_42"][:5])
+
+
+def _diag_heavy(n, count, seed):
+    """Random circuit dominated by diagonal gates (Z S Sdg T Tdg Rz CZ CP CRz)
+    with some H, CX and U between them."""
+    from oracle.oracle import make_ops
+    rng = np.random.default_rng(seed)
+    diag1 = ["Z", "S", "Sdg", "T", "Tdg", "Rz"]
+    diag2 = ["CZ", "CP", "CRz"]
+    gs = [("H", [q]) for q in range(n)]
+    for _ in range(count):
+        r = rng.random()
+        if r < 0.35:
+            g = diag1[int(rng.integers(len(diag1)))]
+            gs.append((g, [int(rng.integers(n))], [float(rng.uniform(0, 2 * math.pi))] if g == "Rz" else []))
+        elif r < 0.8:
+            g = diag2[int(rng.integers(len(diag2)))]
+            a, b = (int(x) for x in rng.choice(n, 2, replace=False))
+            gs.append((g, [a, b], [float(rng.uniform(0, 2 * math.pi))] if g != "CZ" else []))
+        elif r < 0.9:
+            a, b = (int(x) for x in rng.choice(n, 2, replace=False))
+            gs.append(("CX", [a, b]))
+        else:
+            gs.append(("U", [int(rng.integers(n))], rng.uniform(0, 2 * math.pi, 3).tolist()))
+    return make_ops(gs)
+
+
+@pytest.mark.parametrize("n", [5, 6, 7, 12, 13, 15])
+def test_diagonal_runs_qft_pattern(oracle, n):
+    """H on all, CP(pi/2^(j-i)) on every pair, GHZ ladder, Rz layer: the CP
+    run becomes one diagonal pass (low-bit table + per-chunk tables)."""
+    from ket_b200.workloads import qft_ghz_rz
+    ops = qft_ghz_rz(n).to_ops()
+    want = oracle.run(n, ops, fuse=0)
+    for k in (3, 5):
+        got = gpu_run(n, ops, "c128", "greedy", k)
+        assert np.abs(got - want).max() < TOL64, k
+    got = gpu_run(n, ops, "c64", "greedy", 5, True)
+    assert np.abs(got - want).max() < TOL32
+    assert fidelity(got, want) > 1 - FID32
+
+
+@pytest.mark.parametrize("n,seed", [(9, 1), (14, 2), (16, 3)])
+def test_diagonal_heavy_random(oracle, n, seed):
+    ops = _diag_heavy(n, 300, seed)
+    want = oracle.run(n, ops, fuse=0)
+    for fusion, k in [("greedy", 3), ("greedy", 5), ("greedy", 6), ("learned", 5)]:
+        got = gpu_run(n, ops, "c128", fusion, k)
+        assert np.abs(got - want).max() < TOL64, (fusion, k)
+    for tc in (True, False):
+        got = gpu_run(n, ops, "c64", "greedy", 5, tc)
+        assert np.abs(got - want).max() < TOL32
+        assert fidelity(got, want) > 1 - FID32

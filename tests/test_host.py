@@ -98,6 +98,34 @@ def test_plans_on_the_host():
     assert gr["bytes"] < un["bytes"] / 8
 
 
+def test_diagonal_runs_in_the_plan():
+    """The 33-qubit QFT-pattern circuit: the 528 CP gates form one diagonal
+    pass; the brick wall (no diagonal gates) is planned as before."""
+    import ctypes as ct
+
+    import ket_b200 as ket
+    from ket_b200 import _lib
+    from ket_b200.workloads import qft_ghz_rz
+    c = qft_ghz_rz(33)
+    opt = ket.make_options("c64", "greedy", 5, True)
+    st = ket.plan_stats(c, opt)
+    assert st["n_passes"] <= 20 and st["n_gates"] == 627
+    ops = c.to_ops()
+    h = ct.c_void_p()
+    _lib.check(_lib.lib.ketgpu_plan_create(33, ops.ctypes.data, len(ops), ct.byref(opt), ct.byref(h)))
+    kinds = []
+    for i in range(st["n_passes"]):
+        kind, k, tc, b = ct.c_int32(), ct.c_int32(), ct.c_int32(), ct.c_double()
+        _lib.check(_lib.lib.ketgpu_plan_pass_info(h, i, ct.byref(kind), ct.byref(k), ct.byref(tc), ct.byref(b)))
+        kinds.append((kind.value, k.value))
+    _lib.lib.ketgpu_plan_destroy(h)
+    diag = [k for kind, k in kinds if kind == 4]
+    assert diag == [33]
+    # no diagonal runs without fusion, or with ket's own Fuser rule
+    for mode in ("none", "reference"):
+        assert ket.plan_stats(c, ket.make_options("c64", mode))["n_passes"] > 400
+
+
 def test_plan_errors():
     import ket_b200 as ket
     from ket_b200 import _lib
