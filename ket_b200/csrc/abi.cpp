@@ -5,7 +5,11 @@
 // launch, and leaves the caller's current CUDA device unchanged.
 #include <cuda_runtime.h>
 
+#include <immintrin.h>
+
 #include <algorithm>
+#include <atomic>
+#include <barrier>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -209,7 +213,38 @@ struct Pinned {
   }
 };
 
-constexpr uint64_t kChunk = uint64_t{1} << 24;  // amplitudes per staged copy
+constexpr uint64_t kChunk = uint64_t{1} << 24;  // amplitudes per staged upload copy
+
+// complex64 -> complex128 widening of n floats (re, im interleaved).  The
+// AVX-512 form widens 8 floats per instruction and writes with non-temporal
+// stores (no read-for-ownership of the destination lines), which matters
+// because the destination is twice the size of everything else that moves.
+__attribute__((target("avx512f"))) void widen_avx512(const float* src, double* dst, uint64_t n) {
+  uint64_t i = 0;
+  while (i < n && (reinterpret_cast<uintptr_t>(dst + i) & 63)) {
+    dst[i] = (double)src[i];
+    ++i;
+  }
+  for (; i + 8 <= n; i += 8) _mm512_stream_pd(dst + i, _mm512_cvtps_pd(_mm256_loadu_ps(src + i)));
+  for (; i < n; ++i) dst[i] = (double)src[i];
+  _mm_sfence();
+}
+
+void widen_scalar(const float* src, double* dst, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i) dst[i] = (double)src[i];
+}
+
+bool have_avx512() {
+  static const bool v = __builtin_cpu_supports("avx512f");
+  return v;
+}
+
+// Pinned staging for complex64 downloads, kept for the life of the process:
+// three buffers of kDownChunk amplitudes (96 MB).  One download at a time
+// uses it.
+constexpr uint64_t kDownChunk = uint64_t{1} << 22;
+std::mutex g_stage_mu;
+void* g_stage = nullptr;
 
 void download(const State& s, uint64_t first, uint64_t count, double* out) {
   if (s.precision == KETGPU_C128) {
@@ -218,35 +253,60 @@ void download(const State& s, uint64_t first, uint64_t count, double* out) {
     KB_CUDA(cudaStreamSynchronize(s.stream));
     return;
   }
-  const uint64_t chunk = std::min<uint64_t>(kChunk, std::max<uint64_t>(count, 1));
-  Pinned stage(2 * chunk * 8);
-  float2* buf[2] = {static_cast<float2*>(stage.p), static_cast<float2*>(stage.p) + chunk};
-  cudaEvent_t ev[2];
-  KB_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-  KB_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
-  const uint64_t nchunks = (count + chunk - 1) / chunk;
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  if (!g_stage) KB_CUDA(cudaMallocHost(&g_stage, 3 * kDownChunk * 8));
+  float2* buf[3];
+  for (int b = 0; b < 3; ++b) buf[b] = static_cast<float2*>(g_stage) + b * kDownChunk;
+  cudaEvent_t ev[3];
+  for (auto& e : ev) KB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  const uint64_t nchunks = (count + kDownChunk - 1) / kDownChunk;
+  cudaError_t err = cudaSuccess;  // no throw while the workers run
   auto issue = [&](uint64_t c) {
-    const uint64_t lo = c * chunk, len = std::min(chunk, count - lo);
-    KB_CUDA(cudaMemcpyAsync(buf[c & 1], static_cast<const float2*>(s.amps) + first + lo, len * 8,
-                            cudaMemcpyDeviceToHost, s.stream));
-    KB_CUDA(cudaEventRecord(ev[c & 1], s.stream));
+    const uint64_t lo = c * kDownChunk, len = std::min(kDownChunk, count - lo);
+    cudaError_t e = cudaMemcpyAsync(buf[c % 3], static_cast<const float2*>(s.amps) + first + lo, len * 8,
+                                    cudaMemcpyDeviceToHost, s.stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[c % 3], s.stream);
+    if (e != cudaSuccess && err == cudaSuccess) err = e;
   };
-  if (nchunks) issue(0);
+  // Chunk c is widened by every worker while chunks c+1 and c+2 are in
+  // flight.  The workers start once per download and step through the
+  // chunks between two barriers; the calling thread is worker 0 and also
+  // issues the copies.
+  const unsigned nt = count < (uint64_t{1} << 20) ? 1u
+                                                  : std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  const bool wide = have_avx512();
+  auto slice = [&](unsigned t, uint64_t c) {
+    const uint64_t lo = c * kDownChunk, len = std::min(kDownChunk, count - lo);
+    // in floats, rounded to 16 floats (64 bytes of output) per worker
+    const uint64_t nf = 2 * len, per = ((nf + nt - 1) / nt + 15) / 16 * 16;
+    const uint64_t a = std::min(nf, t * per), b = std::min(nf, a + per);
+    if (b > a)
+      (wide ? widen_avx512 : widen_scalar)(reinterpret_cast<const float*>(buf[c % 3]) + a, out + 2 * lo + a, b - a);
+  };
+  std::barrier sync(nt);
+  auto work = [&](unsigned t) {
+    for (uint64_t c = 0; c < nchunks; ++c) {
+      sync.arrive_and_wait();  // chunk c has landed
+      slice(t, c);
+      sync.arrive_and_wait();  // chunk c is consumed
+    }
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+  for (uint64_t c = 0; c < std::min<uint64_t>(2, nchunks); ++c) issue(c);
   for (uint64_t c = 0; c < nchunks; ++c) {
-    KB_CUDA(cudaEventSynchronize(ev[c & 1]));
-    if (c + 1 < nchunks) issue(c + 1);
-    const uint64_t lo = c * chunk, len = std::min(chunk, count - lo);
-    const float2* src = buf[c & 1];
-    double* dst = out + 2 * lo;
-    parallel_chunks(len, [&](uint64_t a, uint64_t b) {
-      for (uint64_t i = a; i < b; ++i) {
-        dst[2 * i] = (double)src[i].x;
-        dst[2 * i + 1] = (double)src[i].y;
-      }
-    });
+    if (err == cudaSuccess) {
+      const cudaError_t e = cudaEventSynchronize(ev[c % 3]);
+      if (e != cudaSuccess) err = e;
+    }
+    if (c + 2 < nchunks && err == cudaSuccess) issue(c + 2);
+    sync.arrive_and_wait();
+    slice(0, c);
+    sync.arrive_and_wait();
   }
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
+  for (auto& x : th) x.join();
+  for (auto& e : ev) cudaEventDestroy(e);
+  check_cuda(err, "download");
 }
 
 void upload(State& s, uint64_t first, uint64_t count, const double* in) {
