@@ -701,6 +701,436 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// complex64 tiled sweeps on packed pairs.  Blackwell's f32x2 instructions
+// (fma.rn.f32x2, mul.rn.f32x2) do two FP32 operations each.  Register slot 0 of a
+// complex64 phase is its pack bit: no gate of the phase targets it with a
+// pair or uses it as a control (the planner guarantees it), so the two
+// amplitudes that differ only in that bit always meet the same coefficients
+// and live in one 64-bit register pair: re = (re_lo, re_hi), im = (im_lo,
+// im_hi).  A thread's 16 amplitudes of a state are 8 such packs of each
+// part; a gate on register slot S (1..3) acts across packs jo and
+// jo | 1 << (S-1).  A diagonal gate may target the pack bit itself (its two
+// phases then form a per-half pack).  Per gate the shared memory holds 16
+// packed coefficients of U (forward) or U^dag (reverse):
+//   [0..7]  c0r c0i c1r c1i c2r c2i c3r c3i, each duplicated in both halves
+//   [8..11] -c0i -c1i -c2i -c3i
+//   [12..14] (c0r, c3r) (c0i, c3i) (-c0i, -c3i): a diagonal on the pack bit
+using f2 = unsigned long long;  // (lo, hi) halves in one 64-bit register pair
+
+__device__ __forceinline__ f2 pk2(float lo, float hi) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void upk2(f2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f2 mul2p(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ float hsum2(f2 v) {
+  float lo, hi;
+  upk2(v, lo, hi);
+  return lo + hi;
+}
+
+struct PackState {
+  f2 r[8], i[8];
+};
+
+// (xr, xi) <- complex phase (pr, pi) times (xr, xi); npi = -pi.
+__device__ __forceinline__ void pk_phase(f2& xr, f2& xi, f2 pr, f2 pi, f2 npi) {
+  const f2 nr = fma2(pr, xr, mul2p(npi, xi));
+  xi = fma2(pr, xi, mul2p(pi, xr));
+  xr = nr;
+}
+
+// 2x2 on packs a, b: (a, b) <- (c0 a + c1 b, c2 a + c3 b).
+template <bool REAL>
+__device__ __forceinline__ void pk_2x2(f2& ar, f2& ai, f2& br, f2& bi, const f2* c) {
+  if (REAL) {
+    const f2 xr = fma2(c[0], ar, mul2p(c[2], br)), xi = fma2(c[0], ai, mul2p(c[2], bi));
+    const f2 yr = fma2(c[4], ar, mul2p(c[6], br)), yi = fma2(c[4], ai, mul2p(c[6], bi));
+    ar = xr, ai = xi, br = yr, bi = yi;
+  } else {
+    const f2 xr = fma2(c[0], ar, fma2(c[8], ai, fma2(c[2], br, mul2p(c[9], bi))));
+    const f2 xi = fma2(c[0], ai, fma2(c[1], ar, fma2(c[2], bi, mul2p(c[3], br))));
+    const f2 yr = fma2(c[4], ar, fma2(c[10], ai, fma2(c[6], br, mul2p(c[11], bi))));
+    const f2 yi = fma2(c[4], ai, fma2(c[5], ar, fma2(c[6], bi, mul2p(c[7], br))));
+    ar = xr, ai = xi, br = yr, bi = yi;
+  }
+}
+
+// Gate bodies, fully specialised at compile time: register slot(s), real or
+// complex matrix, gradient generator (reverse only) and whether some
+// controls are register bits (RC; then each pack is tested against them).
+
+// Swap on outer slot S (1..3): X, CX, CCX.
+template <int S, bool REV, bool RC>
+__device__ __forceinline__ float pk_swap(PackState& a, PackState& l, const TGate& g) {
+  constexpr int so = S - 1;
+  const int cm = g.cm_r >> 1;
+#pragma unroll
+  for (int jo = 0; jo < 8; ++jo) {
+    if (jo & (1 << so)) continue;
+    if (RC && (jo & cm) != cm) continue;
+    const int j1 = jo | (1 << so);
+    f2 t = a.r[jo]; a.r[jo] = a.r[j1]; a.r[j1] = t;
+    t = a.i[jo]; a.i[jo] = a.i[j1]; a.i[j1] = t;
+    if (REV) {
+      t = l.r[jo]; l.r[jo] = l.r[j1]; l.r[j1] = t;
+      t = l.i[jo]; l.i[jo] = l.i[j1]; l.i[j1] = t;
+    }
+  }
+  return 0.f;
+}
+
+// 2x2 on outer slot S.  Reverse: the gradient term Im <l|G|a> first (GEN
+// 1 X, 2 Y, 3 Z), as plus and minus packed sums.
+template <int S, bool REAL, int GEN, bool REV, bool RC>
+__device__ __forceinline__ float pk_pair(PackState& a, PackState& l, const TGate& g, const f2* c) {
+  constexpr int so = S - 1;
+  const int cm = g.cm_r >> 1;
+  f2 plus = 0, minus = 0;
+#pragma unroll
+  for (int jo = 0; jo < 8; ++jo) {
+    if (jo & (1 << so)) continue;
+    if (RC && (jo & cm) != cm) continue;
+    const int j1 = jo | (1 << so);
+    if (REV && GEN == 1) {  // X: (l0r a1i - l0i a1r) + (l1r a0i - l1i a0r)
+      plus = fma2(l.r[jo], a.i[j1], fma2(l.r[j1], a.i[jo], plus));
+      minus = fma2(l.i[jo], a.r[j1], fma2(l.i[j1], a.r[jo], minus));
+    } else if (REV && GEN == 2) {  // Y: (l1r a0r + l1i a0i) - (l0r a1r + l0i a1i)
+      plus = fma2(l.r[j1], a.r[jo], fma2(l.i[j1], a.i[jo], plus));
+      minus = fma2(l.r[jo], a.r[j1], fma2(l.i[jo], a.i[j1], minus));
+    } else if (REV && GEN == 3) {  // Z: (l0r a0i - l0i a0r) - (l1r a1i - l1i a1r)
+      plus = fma2(l.r[jo], a.i[jo], fma2(l.i[j1], a.r[j1], plus));
+      minus = fma2(l.i[jo], a.r[jo], fma2(l.r[j1], a.i[j1], minus));
+    }
+    pk_2x2<REAL>(a.r[jo], a.i[jo], a.r[j1], a.i[j1], c);
+    if (REV) pk_2x2<REAL>(l.r[jo], l.i[jo], l.r[j1], l.i[j1], c);
+  }
+  return (REV && GEN) ? hsum2(plus) - hsum2(minus) : 0.f;
+}
+
+template <int A, int B, bool REV, bool RC>
+__device__ __forceinline__ float pk_swap2(PackState& a, PackState& l, const TGate& g) {
+  constexpr int oa = A - 1, ob = B - 1;
+  const int cm = g.cm_r >> 1;
+#pragma unroll
+  for (int jo = 0; jo < 8; ++jo) {
+    if (!(jo & (1 << oa)) || (jo & (1 << ob))) continue;
+    if (RC && (jo & cm) != cm) continue;
+    const int j1 = jo ^ (1 << oa) ^ (1 << ob);
+    f2 t = a.r[jo]; a.r[jo] = a.r[j1]; a.r[j1] = t;
+    t = a.i[jo]; a.i[jo] = a.i[j1]; a.i[j1] = t;
+    if (REV) {
+      t = l.r[jo]; l.r[jo] = l.r[j1]; l.r[j1] = t;
+      t = l.i[jo]; l.i[jo] = l.i[j1]; l.i[j1] = t;
+    }
+  }
+  return 0.f;
+}
+
+// Diagonal gate.  TS: register slot of the target (1..3), 0 for the pack
+// bit, -1 for a group bit (its value for this thread is read from gbase).
+// Gradient (GEN 3 Z, 4 P11): Im(conj(l) a) per amplitude, weighted +-1 by the
+// target bit (Z) or kept only where it is 1 (P11).
+template <int TS, int GEN, bool REV, bool RC>
+__device__ __forceinline__ float pk_diag(PackState& a, PackState& l, const TGate& g, const f2* c, int gbase) {
+  const int cm = g.cm_r >> 1;
+  const bool gbit = TS < 0 ? ((gbase >> g.tbit) & 1) : false;
+  f2 plus0 = 0, minus0 = 0, plus1 = 0, minus1 = 0;  // target bit 0 / 1
+  f2 pr0 = c[0], pi0 = c[1], npi0 = c[8], pr1 = c[6], pi1 = c[7], npi1 = c[11];
+  if (TS == 0) pr0 = c[12], pi0 = c[13], npi0 = c[14];
+  if (TS < 0 && gbit) pr0 = pr1, pi0 = pi1, npi0 = npi1;
+#pragma unroll
+  for (int jo = 0; jo < 8; ++jo) {
+    if (RC && (jo & cm) != cm) continue;
+    const bool bit = TS > 0 ? ((jo >> (TS - 1)) & 1) : false;  // compile time
+    const f2 pr = bit ? pr1 : pr0, pi = bit ? pi1 : pi0, npi = bit ? npi1 : npi0;
+    if (REV && GEN) {
+      if (!bit) {
+        plus0 = fma2(l.r[jo], a.i[jo], plus0);
+        minus0 = fma2(l.i[jo], a.r[jo], minus0);
+      } else {
+        plus1 = fma2(l.r[jo], a.i[jo], plus1);
+        minus1 = fma2(l.i[jo], a.r[jo], minus1);
+      }
+    }
+    pk_phase(a.r[jo], a.i[jo], pr, pi, npi);
+    if (REV) pk_phase(l.r[jo], l.i[jo], pr, pi, npi);
+  }
+  if (!(REV && GEN)) return 0.f;
+  float s0, s1;
+  if (TS == 0) {  // halves: lo = target bit 0, hi = target bit 1
+    float p0, p1, m0, m1;
+    upk2(plus0, p0, p1);
+    upk2(minus0, m0, m1);
+    s0 = p0 - m0;
+    s1 = p1 - m1;
+  } else if (TS < 0) {  // every element of the thread has target bit gbit
+    const float t = hsum2(plus0) - hsum2(minus0);
+    s0 = gbit ? 0.f : t;
+    s1 = gbit ? t : 0.f;
+  } else {
+    s0 = hsum2(plus0) - hsum2(minus0);
+    s1 = hsum2(plus1) - hsum2(minus1);
+  }
+  return GEN == 3 ? s0 - s1 : s1;
+}
+
+// Flat opcode of a gate, computed once per CTA when the block's gates are
+// staged (the generator counts only in the reverse sweep):
+//   pair   (S-1)*16 + real*8 + gen*2 + rc           0..47
+//   swap   48 + (S-1)*2 + rc                         48..53
+//   swap2  54 + {(1,2):0, (1,3):1, (2,3):2}*2 + rc   54..59
+//   diag   60 + (TS+1)*6 + {0:0, 3:1, 4:2}[gen]*2 + rc   60..89
+__device__ __forceinline__ int pk_opcode(const TGate& g, bool rev) {
+  const int rc = g.cm_r ? 1 : 0;
+  const int gen = rev ? g.gen : 0;
+  switch (g.kind) {
+    case kTPair: return (g.s0 - 1) * 16 + (g.real ? 8 : 0) + gen * 2 + rc;
+    case kTPairSwap: return 48 + (g.s0 - 1) * 2 + rc;
+    case kTSwap2: return 54 + (g.s0 == 1 ? (g.s1 == 2 ? 0 : 1) : 2) * 2 + rc;
+    default: return 60 + (g.tslot + 1) * 6 + (gen == 3 ? 1 : gen == 4 ? 2 : 0) * 2 + rc;
+  }
+}
+
+template <int OP, bool REV>
+__device__ __forceinline__ float pk_exec(PackState& a, PackState& l, const TGate& g, const f2* c, int gbase) {
+  if constexpr (OP < 48) {
+    return pk_pair<OP / 16 + 1, ((OP / 8) & 1) != 0, (OP / 2) & 3, REV, (OP & 1) != 0>(a, l, g, c);
+  } else if constexpr (OP < 54) {
+    return pk_swap<(OP - 48) / 2 + 1, REV, (OP & 1) != 0>(a, l, g);
+  } else if constexpr (OP < 60) {
+    constexpr int w = (OP - 54) / 2;
+    return pk_swap2<w == 2 ? 2 : 1, w == 0 ? 2 : 3, REV, (OP & 1) != 0>(a, l, g);
+  } else {
+    constexpr int t = (OP - 60) / 6, gi = ((OP - 60) % 6) / 2;
+    return pk_diag<t - 1, gi == 0 ? 0 : gi == 1 ? 3 : 4, REV, (OP & 1) != 0>(a, l, g, c, gbase);
+  }
+}
+
+#define KB_PK_CASE(N) \
+  case N: return pk_exec<N, REV>(a, l, g, c, gbase);
+#define KB_PK_CASE10(N)                                                                                    \
+  KB_PK_CASE(N + 0) KB_PK_CASE(N + 1) KB_PK_CASE(N + 2) KB_PK_CASE(N + 3) KB_PK_CASE(N + 4) KB_PK_CASE(N + 5) \
+  KB_PK_CASE(N + 6) KB_PK_CASE(N + 7) KB_PK_CASE(N + 8) KB_PK_CASE(N + 9)
+
+template <bool REV>
+__device__ __forceinline__ float pk_dispatch(int op, PackState& a, PackState& l, const TGate& g, const f2* c,
+                                             int gbase) {
+  switch (op) {
+    KB_PK_CASE10(0) KB_PK_CASE10(10) KB_PK_CASE10(20) KB_PK_CASE10(30) KB_PK_CASE10(40)
+    KB_PK_CASE10(50) KB_PK_CASE10(60) KB_PK_CASE10(70) KB_PK_CASE10(80)
+    default: return 0.f;
+  }
+}
+#undef KB_PK_CASE10
+#undef KB_PK_CASE
+
+// The complex64 form of tile_sweep (same grid, pipeline and partials).
+template <bool REV>
+__global__ void __launch_bounds__(kTileThreads, 1)
+    tile_sweep_c64(float2* __restrict__ psi, float2* __restrict__ lam, uint64_t dim, TileGeom tg,
+                   const TGate* __restrict__ gates, int ngates, const TPhase* __restrict__ phases, int nph,
+                   const float* __restrict__ mats, uint64_t mat_stride, int ngrad, double* __restrict__ partial) {
+  constexpr int TB = TileCfg<float>::TB, RB = TileCfg<float>::RB, TILE = 1 << TB;
+  static_assert(RB == 4, "8 packs of 2 amplitudes per state");
+  constexpr int BUF = (REV ? 2 : 1) * TILE;
+  extern __shared__ __align__(16) unsigned char tsm[];
+  float2* bufs = reinterpret_cast<float2*>(tsm);
+  f2* spk = reinterpret_cast<f2*>(tsm + 2 * BUF * sizeof(float2));  // [gate][16]
+  TGate* sg = reinterpret_cast<TGate*>(spk + 16 * (size_t)ngates);
+  double* acc = reinterpret_cast<double*>(sg + ngates);  // [warp][ngrad]
+  __shared__ uint8_t sop[kMaxBlockGates];
+  __shared__ uint64_t off_lo[64], off_hi[64];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int set = blockIdx.y;
+  float2* s = psi + (uint64_t)set * dim;
+  float2* l = REV ? lam + (uint64_t)set * dim : nullptr;
+
+  if (tid < 128) {
+    const int half = tid >> 6, e = tid & 63;
+    uint64_t off = 0;
+    for (int b = 0; b < 6; ++b) {
+      const int tb = 6 * half + b;
+      if (tb < TB && ((e >> b) & 1)) off |= uint64_t{1} << tg.pos[tb];
+    }
+    (half ? off_hi : off_lo)[e] = off;
+  }
+  for (int i = tid; i < ngates; i += kTileThreads) {
+    const TGate g = gates[i];
+    sg[i] = g;
+    sop[i] = (uint8_t)pk_opcode(g, REV);
+    const float* m = mats + ((uint64_t)g.mat * mat_stride + set) * 8;
+    // U or U^dag, row-major (re, im) of entries 0..3
+    float cr[4], ci[4];
+    if (!REV) {
+      for (int k = 0; k < 4; ++k) cr[k] = m[2 * k], ci[k] = m[2 * k + 1];
+    } else {
+      cr[0] = m[0], ci[0] = -m[1];
+      cr[1] = m[4], ci[1] = -m[5];
+      cr[2] = m[2], ci[2] = -m[3];
+      cr[3] = m[6], ci[3] = -m[7];
+    }
+    f2* c = spk + 16 * i;
+    for (int k = 0; k < 4; ++k) {
+      c[2 * k] = pk2(cr[k], cr[k]);
+      c[2 * k + 1] = pk2(ci[k], ci[k]);
+      c[8 + k] = pk2(-ci[k], -ci[k]);
+    }
+    c[12] = pk2(cr[0], cr[3]);
+    c[13] = pk2(ci[0], ci[3]);
+    c[14] = pk2(-ci[0], -ci[3]);
+    c[15] = 0;
+  }
+  if (REV)
+    for (int i = tid; i < kTileWarps * ngrad; i += kTileThreads) acc[i] = 0.0;
+  __syncthreads();
+
+  auto tile_base = [&](uint64_t t) {
+    uint64_t base = t;
+#pragma unroll
+    for (int b = 0; b < TB; ++b) {
+      const int f = tg.pos[b];
+      base = ((base >> f) << (f + 1)) | (base & ((uint64_t{1} << f) - 1));
+    }
+    return base;
+  };
+  auto prefetch = [&](uint64_t t, float2* buf) {
+    const uint64_t base = tile_base(t);
+#pragma unroll 2
+    for (int r = 0; r < (1 << RB); ++r) {
+      const int e = tid + r * kTileThreads;
+      const uint64_t o = base + (off_lo[e & 63] | off_hi[e >> 6]);
+      tile_cp_async(buf + tphys<float>(e), s + o);
+      if (REV) tile_cp_async(buf + TILE + tphys<float>(e), l + o);
+    }
+  };
+
+  int cur = 0;
+  if (blockIdx.x < tg.n_tiles) prefetch(blockIdx.x, bufs);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  for (uint64_t t = blockIdx.x; t < tg.n_tiles; t += gridDim.x) {
+    float2* sp = bufs + cur * BUF;
+    float2* sl = sp + TILE;
+    if (t + gridDim.x < tg.n_tiles) prefetch(t + gridDim.x, bufs + (cur ^ 1) * BUF);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    __syncthreads();
+    for (int k = 0; k < nph; ++k) {
+      const TPhase P = phases[REV ? nph - 1 - k : k];
+      int rmask = 0;
+#pragma unroll
+      for (int b = 0; b < RB; ++b) rmask |= 1 << P.r[b];
+      int gbase = 0;
+      {
+        int kk = 0;
+#pragma unroll
+        for (int b = 0; b < TB; ++b)
+          if (!((rmask >> b) & 1)) {
+            gbase |= ((tid >> kk) & 1) << b;
+            ++kk;
+          }
+      }
+      const int pg = tphys<float>(gbase);
+      int pb[RB];
+#pragma unroll
+      for (int b = 0; b < RB; ++b) pb[b] = tphys<float>(1 << P.r[b]);
+      PackState A, L;
+#pragma unroll
+      for (int jo = 0; jo < 8; ++jo) {
+        int a0 = pg;
+#pragma unroll
+        for (int b = 1; b < RB; ++b)
+          if (jo & (1 << (b - 1))) a0 ^= pb[b];
+        const int a1 = a0 ^ pb[0];
+        const float2 x = sp[a0], y = sp[a1];
+        A.r[jo] = pk2(x.x, y.x);
+        A.i[jo] = pk2(x.y, y.y);
+        if (REV) {
+          const float2 u = sl[a0], v = sl[a1];
+          L.r[jo] = pk2(u.x, v.x);
+          L.i[jo] = pk2(u.y, v.y);
+        }
+      }
+      for (int c = 0; c < P.count; ++c) {
+        const int gi = REV ? P.first + P.count - 1 - c : P.first + c;
+        const TGate g = sg[gi];
+        float part = 0.f;
+        if ((gbase & g.cm_g) == g.cm_g) part = pk_dispatch<REV>(sop[gi], A, L, g, spk + 16 * gi, gbase);
+        if (REV && g.grad >= 0) {
+          double v = (double)part;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) acc[warp * ngrad + g.grad] += v;
+        }
+      }
+      {
+        // addresses again from a fresh read of the phase record (not held
+        // in registers across the gates)
+        unsigned rw;
+        asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(rw) : "l"(&phases[REV ? nph - 1 - k : k]));
+        const int pg2 = tphys<float>(gbase);
+        int pb2[RB];
+#pragma unroll
+        for (int b = 0; b < RB; ++b) pb2[b] = tphys<float>(1 << ((rw >> (8 * b)) & 0xff));
+#pragma unroll
+        for (int jo = 0; jo < 8; ++jo) {
+          int a0 = pg2;
+#pragma unroll
+          for (int b = 1; b < RB; ++b)
+            if (jo & (1 << (b - 1))) a0 ^= pb2[b];
+          const int a1 = a0 ^ pb2[0];
+          float xr, yr, xi, yi;
+          upk2(A.r[jo], xr, yr);
+          upk2(A.i[jo], xi, yi);
+          sp[a0] = make_float2(xr, xi);
+          sp[a1] = make_float2(yr, yi);
+          if (REV) {
+            upk2(L.r[jo], xr, yr);
+            upk2(L.i[jo], xi, yi);
+            sl[a0] = make_float2(xr, xi);
+            sl[a1] = make_float2(yr, yi);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    {
+      const uint64_t base = tile_base(t);
+      const volatile uint64_t* vlo = off_lo;
+      const volatile uint64_t* vhi = off_hi;
+#pragma unroll 2
+      for (int r = 0; r < (1 << RB); ++r) {
+        const int e = tid + r * kTileThreads;
+        const uint64_t o = base + (vlo[e & 63] | vhi[e >> 6]);
+        s[o] = sp[tphys<float>(e)];
+        if (REV) l[o] = sl[tphys<float>(e)];
+      }
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  if (REV)
+    for (int g = tid; g < ngrad; g += kTileThreads) {
+      double v = 0.0;
+      for (int w = 0; w < kTileWarps; ++w) v += acc[w * ngrad + g];
+      partial[((uint64_t)set * ngrad + g) * gridDim.x + blockIdx.x] = v;
+    }
+}
+
 // Host plan of the tiled sweeps.
 struct TBlock {
   TileGeom geom;
@@ -771,6 +1201,7 @@ template <typename R>
 TilePlan plan_tiles(int n, const ketgpu_op* ops, const std::vector<int>& gate_ops, const std::vector<int>& layer_of,
                     const std::vector<GateGeom>& geo, const std::vector<uint8_t>& real) {
   constexpr int TB = TileCfg<R>::TB, RB = TileCfg<R>::RB;
+  constexpr bool kPacked = sizeof(R) == 4;  // complex64 sweeps pack pairs of amplitudes
   TilePlan tp;
   const int G = (int)gate_ops.size();
   std::vector<uint64_t> qmask(G);
@@ -858,23 +1289,51 @@ TilePlan plan_tiles(int n, const ketgpu_op* ops, const std::vector<int>& gate_op
       b.gate_first = (int)tp.gates.size();
       b.phase_first = (int)tp.phases.size();
       size_t k0 = 0;
+      const int all_bits = (1 << TB) - 1;
       while (k0 < take.size()) {
         int rmask = 0;
         size_t k1 = k0;
-        for (; k1 < take.size(); ++k1) {
-          int need = 0;
-          for (int t = 0; t < top[k1].ntargets; ++t) need |= 1 << top[k1].targets[t];
-          if (__builtin_popcount(rmask | need) > RB) break;
-          rmask |= need;
-        }
-        for (int t = 0; t < TB && __builtin_popcount(rmask) < RB; ++t) rmask |= 1 << t;
         TPhase ph{};
         int slot_of[12];
-        for (int t = 0, k = 0; t < TB; ++t)
-          if ((rmask >> t) & 1) {
-            ph.r[k] = (uint8_t)t;
-            slot_of[t] = k++;
+        if (kPacked) {
+          // complex64: register slot 0 is the pack bit, a tile bit that no
+          // gate of the phase targets (pair kinds) or uses as a control;
+          // the targets take at most the other RB - 1 slots
+          int forbid = 0;
+          for (; k1 < take.size(); ++k1) {
+            int need = 0;
+            for (int t = 0; t < top[k1].ntargets; ++t) need |= 1 << top[k1].targets[t];
+            const int f = forbid | need | top[k1].cmask;
+            if (__builtin_popcount(rmask | need) > RB - 1 || (f & all_bits) == all_bits) break;
+            rmask |= need;
+            forbid = f;
           }
+          int pack = 0;
+          while ((forbid >> pack) & 1) ++pack;
+          for (int t = 0; t < TB && __builtin_popcount(rmask) < RB - 1; ++t)
+            if (t != pack) rmask |= 1 << t;
+          ph.r[0] = (uint8_t)pack;
+          slot_of[pack] = 0;
+          for (int t = 0, k = 1; t < TB; ++t)
+            if ((rmask >> t) & 1) {
+              ph.r[k] = (uint8_t)t;
+              slot_of[t] = k++;
+            }
+          rmask |= 1 << pack;
+        } else {
+          for (; k1 < take.size(); ++k1) {
+            int need = 0;
+            for (int t = 0; t < top[k1].ntargets; ++t) need |= 1 << top[k1].targets[t];
+            if (__builtin_popcount(rmask | need) > RB) break;
+            rmask |= need;
+          }
+          for (int t = 0; t < TB && __builtin_popcount(rmask) < RB; ++t) rmask |= 1 << t;
+          for (int t = 0, k = 0; t < TB; ++t)
+            if ((rmask >> t) & 1) {
+              ph.r[k] = (uint8_t)t;
+              slot_of[t] = k++;
+            }
+        }
         ph.first = (int)tp.gates.size() - b.gate_first;  // relative to the block's first gate
         ph.count = (int)(k1 - k0);
         for (size_t k = k0; k < k1; ++k) {
@@ -943,6 +1402,32 @@ int gen_of(int type) {
     case KETGPU_CP: return 4;
     default: return 0;
   }
+}
+
+// Dynamic shared memory of one tiled sweep launch (see the kernels).
+template <typename R>
+size_t tile_smem(bool rev, int ngates, int ngrad) {
+  using T = typename C2T<R>::T;
+  const size_t tiles = (rev ? 4 : 2) * (size_t{1} << TileCfg<R>::TB) * sizeof(T);
+  const size_t per_gate = sizeof(R) == 4 ? 16 * sizeof(f2) + sizeof(TGate) : sizeof(TGate) + 8 * sizeof(R);
+  return tiles + (size_t)ngates * per_gate + (rev ? (size_t)kTileWarps * ngrad * 8 : 0);
+}
+
+template <typename R, bool REV>
+void launch_tile(dim3 grid, cudaStream_t st, typename C2T<R>::T* psi, typename C2T<R>::T* lam, uint64_t dim,
+                 const TBlock& b, const TGate* gates, const TPhase* phases, const R* mats, uint64_t chunk,
+                 double* partial) {
+  const int ngrad = REV ? (int)b.grad_gate.size() : 0;
+  const size_t smem = tile_smem<R>(REV, b.n_gates, ngrad);
+  if constexpr (sizeof(R) == 4)
+    tile_sweep_c64<REV><<<grid, kTileThreads, smem, st>>>(psi, lam, dim, b.geom, gates + b.gate_first, b.n_gates,
+                                                          phases + b.phase_first, b.n_phases, mats, chunk, ngrad,
+                                                          partial);
+  else
+    tile_sweep<R, REV><<<grid, kTileThreads, smem, st>>>(psi, lam, dim, b.geom, gates + b.gate_first, b.n_gates,
+                                                         phases + b.phase_first, b.n_phases, mats, chunk, ngrad,
+                                                         partial);
+  count_launch();
 }
 
 template <typename R>
@@ -1077,11 +1562,15 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
     }
     static bool attr_set[2] = {false, false};
     if (!attr_set[sizeof(R) == 8]) {
-      const int per_gate = (int)(sizeof(TGate) + 8 * sizeof(R));
-      const int smem_rev = 4 * (1 << TB) * (int)sizeof(T) + kMaxBlockGates * per_gate + kTileWarps * kMaxBlockGrads * 8;
-      const int smem_fwd = 2 * (1 << TB) * (int)sizeof(T) + kMaxBlockGates * per_gate;
-      KB_CUDA(cudaFuncSetAttribute(tile_sweep<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rev));
-      KB_CUDA(cudaFuncSetAttribute(tile_sweep<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fwd));
+      const int smem_rev = (int)tile_smem<R>(true, kMaxBlockGates, kMaxBlockGrads);
+      const int smem_fwd = (int)tile_smem<R>(false, kMaxBlockGates, 0);
+      if constexpr (sizeof(R) == 4) {
+        KB_CUDA(cudaFuncSetAttribute(tile_sweep_c64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rev));
+        KB_CUDA(cudaFuncSetAttribute(tile_sweep_c64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fwd));
+      } else {
+        KB_CUDA(cudaFuncSetAttribute(tile_sweep<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rev));
+        KB_CUDA(cudaFuncSetAttribute(tile_sweep<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_fwd));
+      }
       attr_set[sizeof(R) == 8] = true;
     }
   }
@@ -1118,11 +1607,8 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
       for (const TBlock& b : tp.blocks) {
         while (next_ck < n_ckpt && next_ck * m <= b.layer) store_ck();
         dim3 grid((unsigned)gx, (unsigned)nb);
-        const size_t smem = 2 * (size_t{1} << TB) * sizeof(T) + (size_t)b.n_gates * (sizeof(TGate) + 8 * sizeof(R));
-        tile_sweep<R, false><<<grid, kTileThreads, smem, st>>>(
-            psi.as<T>(), nullptr, dim, b.geom, d_tgates->as<TGate>() + b.gate_first, b.n_gates,
-            d_tphases->as<TPhase>() + b.phase_first, b.n_phases, mats_t.as<R>(), chunk, 0, nullptr);
-        count_launch();
+        launch_tile<R, false>(grid, st, psi.as<T>(), nullptr, dim, b, d_tgates->as<TGate>(), d_tphases->as<TPhase>(),
+                              mats_t.as<R>(), chunk, nullptr);
       }
     } else {
       for (size_t gi = 0; gi < G; ++gi) {
@@ -1151,15 +1637,9 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
         if (bi + 1 < B && tp.blocks[bi + 1].layer / m != seg && seg + 1 < n_ckpt)
           KB_CUDA(cudaMemcpyAsync(psi.p, ck.as<T>() + (size_t)(seg + 1) * chunk * dim, dim * sizeof(T) * nb,
                                   cudaMemcpyDeviceToDevice, st));
-        const int ngrad = (int)b.grad_gate.size();
         dim3 grid((unsigned)gx, (unsigned)nb);
-        const size_t smem = 4 * (size_t{1} << TB) * sizeof(T) +
-                            (size_t)b.n_gates * (sizeof(TGate) + 8 * sizeof(R)) + (size_t)kTileWarps * ngrad * 8;
-        tile_sweep<R, true><<<grid, kTileThreads, smem, st>>>(
-            psi.as<T>(), lam.as<T>(), dim, b.geom, d_tgates->as<TGate>() + b.gate_first, b.n_gates,
-            d_tphases->as<TPhase>() + b.phase_first, b.n_phases, mats_t.as<R>(), chunk, ngrad,
-            part.as<double>() + b.part_off);
-        count_launch();
+        launch_tile<R, true>(grid, st, psi.as<T>(), lam.as<T>(), dim, b, d_tgates->as<TGate>(),
+                             d_tphases->as<TPhase>(), mats_t.as<R>(), chunk, part.as<double>() + b.part_off);
       }
     } else {
       for (size_t gi = G; gi-- > 0;) {

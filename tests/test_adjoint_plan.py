@@ -221,6 +221,16 @@ def _random_circuit(n, count, seed, barriers=3):
 def test_tiled_plan_reproduces_the_oracle(oracle, prec, n, seed):
     ops, pidx, npar = _random_circuit(n, 90, seed)
     blocks = _describe(n, ops, pidx, prec)
+    if prec == "c64":
+        # complex64 phases keep register slot 0 for the pack bit: no pair gate
+        # targets it and no gate uses it as a control
+        for b in blocks:
+            for g in b["gates"]:
+                assert g["cm_r"] & 1 == 0
+                if g["kind"] in (0, 1):
+                    assert g["s0"] >= 1
+                if g["kind"] == 2:
+                    assert g["s0"] >= 1 and g["s1"] >= 1
     # every unitary op is in exactly one block, once
     seen = [g["op"] for b in blocks for g in b["gates"]]
     assert sorted(seen) == [i for i in range(len(ops)) if ops[i]["type"] != CODE["Barrier"]]
@@ -272,4 +282,4 @@ def test_ansatz_layer_needs_three_tiles_at_24_qubits():
     circ, pidx = variational_ansatz(24, 2)
     blocks = _describe(24, circ.to_ops(), pidx, "c64")
     assert len(blocks) == 6
-    assert all(len(b["phases"]) <= 3 for b in blocks)
+    assert all(len(b["phases"]) <= 4 for b in blocks)
