@@ -72,7 +72,7 @@ struct TcGeom {
   int m_low;          // tile qubits 0..m_low-1 form the low run
   int nh;             // tile qubits above the low run
   int hpos[16];
-  int direct;         // qubits 0..4 are group bits: the epilogue stores from registers
+  int direct;         // the epilogue stores from registers (see launch_fused_tc)
   uint64_t cdep[32];  // offset of target combination c from its group's amplitude
   uint64_t n_tiles;
 };
@@ -378,9 +378,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int q = warp & 3;
     const int row = 32 * q + lane;
     if (g.direct) {
-      // TMEM lane = group `row`; neighbouring lanes hold neighbouring
-      // amplitudes (qubits 0..4 are group bits), so each 8-byte store of a
-      // warp covers 256 contiguous bytes.
+      // TMEM lane = group `row`; the lanes of a warp vary the five lowest
+      // group bits, all within qubits 0..5, so a warp's 8-byte stores land
+      // within 512 contiguous bytes.
       uint64_t gdep = 0;
       for (int jb = 0, gb = 0; jb < Cfg::TB; ++jb)
         if (!g.is_target[jb]) {
@@ -505,9 +505,17 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
     }
   g.m_low = 0;
   while (g.m_low < Cfg::TB && g.tile_pos[g.m_low] == g.m_low) ++g.m_low;
-  g.direct = 1;
-  for (int q = 0; q < 5; ++q)
-    if (g.tile_pos[q] != q || g.is_target[q]) g.direct = 0;
+  // Direct stores from TMEM (lane t = group t) when qubit 0 is a group bit
+  // and the five lowest group bits lie within qubits 0..5: a warp's 32
+  // stores then fill 32-byte sectors within 512 contiguous bytes.  Otherwise
+  // (qubit 0 a target, or the lanes spread thin) the output is staged
+  // through shared memory and written in 16-byte words.
+  {
+    int seen = 0, fifth = 64;
+    for (int b = 0; b < Cfg::TB && seen < 5; ++b)
+      if (!g.is_target[b] && ++seen == 5) fifth = g.tile_pos[b];
+    g.direct = (!g.is_target[0] && g.tile_pos[0] == 0 && fifth <= 5) ? 1 : 0;
+  }
   for (int c = 0; c < (1 << p.k); ++c) {
     uint64_t d = 0;
     for (int b = 0; b < p.k; ++b)

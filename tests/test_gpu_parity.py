@@ -85,9 +85,12 @@ def _block_circuit(n, qubits, seed, depth=30):
     return make_ops(gs)
 
 
+# one target among qubits 0..5 with qubit 0 a group bit ("q1tgt5", "q2tgt5",
+# "q3tgt4") takes the direct-store epilogue, like the blocks above qubit 4
 TARGETS = {
     "low5": [0, 1, 2, 3, 4], "high5": None, "mixed5": [0, 3, 7, 11, 13], "spread5": [1, 5, 8, 12, 15],
-    "low4": [0, 1, 2, 3], "mixed4": [2, 6, 9, 14], "high4": None,
+    "q1tgt5": [1, 6, 9, 12, 14], "q2tgt5": [2, 7, 9, 11, 13],
+    "low4": [0, 1, 2, 3], "mixed4": [2, 6, 9, 14], "high4": None, "q3tgt4": [3, 7, 10, 14],
 }
 
 
