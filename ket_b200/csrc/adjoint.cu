@@ -237,6 +237,74 @@ __global__ void __launch_bounds__(kAThreads)
   }
 }
 
+// The same with the terms in shared memory, the phase i^q folded into a
+// complex coefficient, and eight gathers in flight per thread.  Terms:
+// flip, sign mask, coefficient (re, im); at most kHamSmemTerms.
+constexpr int kHamSmemTerms = 1024;
+struct HamTerm {
+  uint64_t flip, sign;
+  double cr, ci;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kAThreads)
+    ham_apply_smem(const typename C2T<R>::T* __restrict__ psi, typename C2T<R>::T* __restrict__ lam, uint64_t dim,
+                   const HamTerm* __restrict__ terms, int nterms, double* __restrict__ partial) {
+  using T = typename C2T<R>::T;
+  __shared__ double sh[32];
+  extern __shared__ __align__(16) unsigned char hsm[];
+  HamTerm* st = reinterpret_cast<HamTerm*>(hsm);
+  for (int i = threadIdx.x; i < nterms; i += blockDim.x) st[i] = terms[i];
+  __syncthreads();
+  const T* s = psi + (uint64_t)blockIdx.y * dim;
+  T* l = lam + (uint64_t)blockIdx.y * dim;
+  double e = 0.0;
+  for (uint64_t y = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; y < dim;
+       y += (uint64_t)gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    int t = 0;
+    for (; t + 8 <= nterms; t += 8) {
+      T a[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) a[u] = s[y ^ st[t + u].flip];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const HamTerm& h = st[t + u];
+        const double ar = a[u].x, ai = a[u].y;
+        const bool neg = __popcll((y ^ h.flip) & h.sign) & 1;
+        const double cr = neg ? -h.cr : h.cr, ci = neg ? -h.ci : h.ci;
+        re += cr * ar - ci * ai;
+        im += cr * ai + ci * ar;
+      }
+    }
+    for (; t < nterms; ++t) {
+      const HamTerm& h = st[t];
+      const T a = s[y ^ h.flip];
+      const double ar = a.x, ai = a.y;
+      const bool neg = __popcll((y ^ h.flip) & h.sign) & 1;
+      const double cr = neg ? -h.cr : h.cr, ci = neg ? -h.ci : h.ci;
+      re += cr * ar - ci * ai;
+      im += cr * ai + ci * ar;
+    }
+    T out;
+    out.x = (R)re;
+    out.y = (R)im;
+    l[y] = out;
+    const T p = s[y];
+    e += (double)p.x * re + (double)p.y * im;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+  if (lane == 0) sh[warp] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[w];
+    partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = v;
+  }
+}
+
 template <typename R>
 __global__ void ground_batch(typename C2T<R>::T* states, uint64_t dim) {
   typename C2T<R>::T one;
@@ -1488,6 +1556,30 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
     std::memcpy(h.data() + 20 * T_, coeffs, 8 * T_);
     KB_CUDA(cudaMemcpyAsync(hmeta.p, h.data(), h.size(), cudaMemcpyHostToDevice, st));
   }
+  // the terms with i^q folded into the coefficient, for ham_apply_smem
+  std::unique_ptr<DevBuf> d_ham;
+  if (T_ <= kHamSmemTerms) {
+    std::vector<HamTerm> ht(T_);
+    for (int t = 0; t < T_; ++t) {
+      const double c = coeffs[t];
+      ht[t].flip = flip[t];
+      ht[t].sign = sign[t];
+      switch (phq[t] & 3) {  // i^q
+        case 0: ht[t].cr = c, ht[t].ci = 0.0; break;
+        case 1: ht[t].cr = 0.0, ht[t].ci = c; break;
+        case 2: ht[t].cr = -c, ht[t].ci = 0.0; break;
+        default: ht[t].cr = 0.0, ht[t].ci = -c; break;
+      }
+    }
+    d_ham = std::make_unique<DevBuf>(sizeof(HamTerm) * std::max(T_, 1));
+    KB_CUDA(cudaMemcpyAsync(d_ham->p, ht.data(), sizeof(HamTerm) * T_, cudaMemcpyHostToDevice, st));
+    static bool ham_attr[2] = {false, false};
+    if (!ham_attr[sizeof(R) == 8]) {
+      KB_CUDA(cudaFuncSetAttribute(ham_apply_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(HamTerm) * kHamSmemTerms)));
+      ham_attr[sizeof(R) == 8] = true;
+    }
+  }
   const uint64_t* d_flip = hmeta.as<uint64_t>();
   const uint64_t* d_sign = d_flip + T_;
   const int* d_q = reinterpret_cast<const int*>(d_sign + T_);
@@ -1623,8 +1715,12 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
     // lambda = H psi and <H>
     {
       dim3 grid((unsigned)blocks, (unsigned)nb);
-      ham_apply<R><<<grid, kAThreads, 0, st>>>(psi.as<T>(), lam.as<T>(), dim, d_flip, d_sign, d_q, d_coef, T_,
-                                               d_ham_part);
+      if (T_ <= kHamSmemTerms)
+        ham_apply_smem<R><<<grid, kAThreads, sizeof(HamTerm) * T_, st>>>(psi.as<T>(), lam.as<T>(), dim,
+                                                                         d_ham->as<HamTerm>(), T_, d_ham_part);
+      else
+        ham_apply<R><<<grid, kAThreads, 0, st>>>(psi.as<T>(), lam.as<T>(), dim, d_flip, d_sign, d_q, d_coef, T_,
+                                                 d_ham_part);
       count_launch();
     }
     // reverse sweep; at the last gate (block) of each segment, walking

@@ -189,10 +189,18 @@ __global__ void __launch_bounds__(kDiagThreads)
     }
     __syncthreads();
     T* sb = s + (h << L);
-#pragma unroll 4
-    for (int e = tid; e < CH; e += kDiagThreads) {
-      const T f = cmul(cmul(t1[e & 63], t2[e >> 6]), q[e]);
-      sb[e] = cmul(sb[e], f);
+    // all of the thread's amplitudes in flight before any arithmetic
+    constexpr int kPer = (1 << kDiagLowBits) / kDiagThreads;
+    T v[kPer];
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+      const int e = tid + r * kDiagThreads;
+      if (e < CH) v[r] = sb[e];
+    }
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+      const int e = tid + r * kDiagThreads;
+      if (e < CH) sb[e] = cmul(v[r], cmul(cmul(t1[e & 63], t2[e >> 6]), q[e]));
     }
   }
 }

@@ -256,6 +256,10 @@ double fused_cost_static(int k, int precision, bool tensor) {
   return k <= 4 ? 1.0 : (k == 5 ? 1.45 : 2.9);
 }
 
+// Predicted gain (fraction of the greedy plan's predicted time) the learned
+// planner needs before it departs from the greedy plan.
+constexpr double kLearnedMargin = 0.02;
+
 bool block_on_tensor_cores(int n, int k, const PlanOptions& opt) {
   return opt.precision == KETGPU_C64 && opt.tensor && tc_supported(k) && n >= k + 7;
 }
@@ -403,6 +407,15 @@ void emit_fused(Plan& plan, int n, const ketgpu_op* ops, const Block& b, const P
   for (int gi : b.gates) gs.push_back(&ops[gi]);
   std::vector<int> qs = b.qubits;
   std::sort(qs.begin(), qs.end());
+  // complex64 on the tensor cores: a 2- or 3-qubit block is padded to 4
+  // qubits (identity on the highest free qubits, so the block's group bits
+  // stay low) and runs at HBM speed instead of on the SIMT block kernel.
+  if (qs.size() >= 2 && qs.size() < 4 && !block_on_tensor_cores(n, (int)qs.size(), opt) &&
+      block_on_tensor_cores(n, 4, opt)) {
+    for (int q = n - 1; q >= 0 && qs.size() < 4; --q)
+      if (std::find(qs.begin(), qs.end(), q) == qs.end()) qs.push_back(q);
+    std::sort(qs.begin(), qs.end());
+  }
   const int k = (int)qs.size();
   std::vector<cplx> mat = block_matrix(gs, qs.data(), k);
   Pass p;
@@ -520,9 +533,10 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
       // fused and as its separate gates by the cost model in one batched
       // inference; the partition with the least predicted time wins, each
       // block taking its cheaper form.
-      const int kmax_cap = std::max(2, std::min(6, opt.max_k + 1));
+      const int kmin_cand = std::min(3, std::max(1, opt.max_k));
+      const int kmax_cap = std::max(kmin_cand, std::min(6, opt.max_k + 1));
       std::vector<std::vector<Block>> cands;
-      for (int kc = 3; kc <= kmax_cap; ++kc) cands.push_back(grow_blocks(n, ops, seg, kc, true));
+      for (int kc = kmin_cand; kc <= kmax_cap; ++kc) cands.push_back(grow_blocks(n, ops, seg, kc, true));
       std::vector<float> rows;
       float fr[kFeatures];
       // single-gate rows, one per gate of the segment
@@ -536,8 +550,16 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
       std::vector<std::vector<size_t>> fused_row(cands.size());
       for (size_t c = 0; c < cands.size(); ++c)
         for (const Block& b : cands[c]) {
-          if (b.diag) {  // a Diagonal pass: scored as one full-state pass of its gates
-            fused_row[c].push_back(0);
+          if (b.diag) {
+            // A Diagonal pass streams the whole state once: scored as the
+            // model's time of a dense one-qubit pass on the run's top qubit.
+            ketgpu_op proxy{};
+            proxy.type = KETGPU_U;
+            proxy.nq = 1;
+            proxy.q[0] = b.qubits.back();
+            pass_features(n, opt.precision, {&proxy}, {proxy.q[0]}, false, false, fr);
+            fused_row[c].push_back(rows.size() / kFeatures);
+            rows.insert(rows.end(), fr, fr + kFeatures);
             continue;
           }
           std::vector<const ketgpu_op*> gs;
@@ -558,6 +580,7 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
           const Block& b = cands[c][bi];
           if (b.diag) {
             choice[c].push_back(2);
+            tot += us[fused_row[c][bi]];
             continue;
           }
           double sep = 0;
@@ -571,6 +594,35 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
           best_t = tot;
           best = c;
         }
+      }
+      // The greedy plan (growth at max_k, static fuse rule), scored by the
+      // same model: the learned choice replaces it only when the model
+      // predicts a clear gain, so model error on near-equal plans cannot
+      // make the learned plan slower than greedy.
+      const size_t gk = (size_t)(std::max(kmin_cand, std::min(opt.max_k, kmax_cap)) - kmin_cand);
+      double greedy_t = 0;
+      std::vector<char> greedy_choice;
+      for (size_t bi = 0; bi < cands[gk].size(); ++bi) {
+        const Block& b = cands[gk][bi];
+        char ch;
+        if (b.diag) {
+          ch = 2;
+          greedy_t += us[fused_row[gk][bi]];
+        } else {
+          double sep = 0, frac = 0;
+          for (int gi : b.gates) {
+            sep += us[single_row[gi]];
+            frac += gate_traffic_fraction(ops[gi]);
+          }
+          ch = b.gates.size() > 1 && fused_cost_static((int)b.qubits.size(), opt.precision, opt.tensor) < frac;
+          greedy_t += ch ? us[fused_row[gk][bi]] : sep;
+        }
+        greedy_choice.push_back(ch);
+      }
+      if (!(best_t < (1.0 - kLearnedMargin) * greedy_t)) {
+        best = gk;
+        best_t = greedy_t;
+        choice[gk] = greedy_choice;
       }
       predicted += best_t;
       for (size_t bi = 0; bi < cands[best].size(); ++bi) {

@@ -168,6 +168,19 @@ def corpus(count: int = 2000, seed: int = 2024, nmin: int = 22, nmax: int = 32, 
             for _ in range(count)]
 
 
+def plan_signature(plan: Plan) -> bytes:
+    """Pass kinds, sizes, bytes and cost-model features of every pass: equal
+    for two plans that apply the same passes."""
+    import ctypes as ct
+    parts = []
+    for i in range(int(plan.stats()["n_passes"])):
+        kind, k, tc, b = ct.c_int32(), ct.c_int32(), ct.c_int32(), ct.c_double()
+        check(lib.ketgpu_plan_pass_info(plan._h, i, ct.byref(kind), ct.byref(k), ct.byref(tc), ct.byref(b)))
+        parts.append(np.array([kind.value, k.value, tc.value, b.value], dtype=np.float64).tobytes())
+        parts.append(pass_features(plan, i).tobytes())
+    return b"".join(parts)
+
+
 def plan_time_ms(circuit: Circuit, fusion: str, k: int = 5, reps: int = 1) -> Tuple[float, Plan]:
     plan = Plan(circuit.n_qubits, circuit.to_ops(), make_options("c64", fusion, k, True))
     st = _state(circuit.n_qubits)
@@ -187,6 +200,7 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     ap.add_argument("--out", default="gpurun_out/planner.json")
     ap.add_argument("--save", default=DEFAULT_MODEL)
     ap.add_argument("--nmax", type=int, default=32)
+    ap.add_argument("--load", default=None, help="evaluate this trained model (skips measuring and training)")
     args = ap.parse_args(argv)
 
     circs = corpus(args.train + args.eval, nmax=args.nmax)
@@ -196,6 +210,8 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     measure_passes(w)
     t0 = time.time()
     X, Y = [], []
+    if args.load:
+        train_spec = []
     for j, (n, d, s) in enumerate(train_spec):
         c = random_mixed(n, d, seed=s)
         sub = Circuit(n)
@@ -206,20 +222,26 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
         if j % 100 == 0:
             print(f"measured {j}/{len(train_spec)} circuits, {sum(len(a) for a in X)} rows, "
                   f"{time.time() - t0:.0f} s", flush=True)
-    X = np.concatenate(X)
-    Y = np.concatenate(Y)
     t_measure = time.time() - t0
-    os.makedirs(os.path.dirname(args.out) or ".", exist_ok=True)
-    np.savez_compressed(os.path.splitext(args.out)[0] + "_rows.npz", X=X, Y=Y)
-    model = CostModel(seed=7)
-    loss0 = float(np.mean((model.forward(X) - Y) ** 2))
-    t1 = time.time()
-    loss = model.train(X, Y, steps=args.steps, minibatch=512, lr=2e-3)
-    loss = model.train(X, Y, steps=args.steps // 2, minibatch=512, lr=5e-4)
-    t_train = time.time() - t1
-    pred = model.forward(X)
-    train_rmse = float(np.sqrt(np.mean((pred - Y) ** 2)))
-    model.save(args.save)
+    if args.load:
+        model = CostModel.load(args.load)
+        X = np.zeros((0, NF), dtype=np.float32)
+        loss0 = loss = train_rmse = None
+        t_train = 0.0
+    else:
+        X = np.concatenate(X)
+        Y = np.concatenate(Y)
+        os.makedirs(os.path.dirname(args.out) or ".", exist_ok=True)
+        np.savez_compressed(os.path.splitext(args.out)[0] + "_rows.npz", X=X, Y=Y)
+        model = CostModel(seed=7)
+        loss0 = float(np.mean((model.forward(X) - Y) ** 2))
+        t1 = time.time()
+        loss = model.train(X, Y, steps=args.steps, minibatch=512, lr=2e-3)
+        loss = model.train(X, Y, steps=args.steps // 2, minibatch=512, lr=5e-4)
+        t_train = time.time() - t1
+        pred = model.forward(X)
+        train_rmse = float(np.sqrt(np.mean((pred - Y) ** 2)))
+        model.save(args.save)
 
     # held-out evaluation
     rng = np.random.default_rng(99)
@@ -229,14 +251,31 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     Xe, Ye = [], []
     for i, (n, d, s) in enumerate(eval_spec):
         c = random_mixed(n, d, seed=s)
+        # plans are built first, then timed in an order that alternates from
+        # circuit to circuit (the plan timed second runs on a warmer GPU)
         CostModel.detach()
-        t_greedy, p_greedy = plan_time_ms(c, "greedy")
+        p_greedy = Plan(n, c.to_ops(), make_options("c64", "greedy", 5, True))
         model.attach()
-        t_learned, p_learned = plan_time_ms(c, "learned")
+        p_learned = Plan(n, c.to_ops(), make_options("c64", "learned", 5, True))
+        CostModel.detach()
+        st_ = _state(n)
+        if i % 2 == 0:
+            t_greedy = float(timed_execute(p_greedy, st_).sum())
+            t_learned = float(timed_execute(p_learned, st_).sum())
+        else:
+            t_learned = float(timed_execute(p_learned, st_).sum())
+            t_greedy = float(timed_execute(p_greedy, st_).sum())
+        same = plan_signature(p_greedy) == plan_signature(p_learned)
+        if not same:  # two more alternating timings of each plan, best of three
+            st = _state(n)
+            for _ in range(2):
+                t_greedy = min(t_greedy, float(timed_execute(p_greedy, st).sum()))
+                t_learned = min(t_learned, float(timed_execute(p_learned, st).sum()))
         pred_learned = float(p_learned.stats()["predicted_us"]) / 1e3
         row = {"n": n, "depth": d, "seed": s, "gates": int(p_greedy.stats()["n_gates"]),
                "greedy_ms": t_greedy, "learned_ms": t_learned, "learned_pred_ms": pred_learned,
-               "greedy_passes": int(p_greedy.stats()["n_passes"]), "learned_passes": int(p_learned.stats()["n_passes"])}
+               "greedy_passes": int(p_greedy.stats()["n_passes"]), "learned_passes": int(p_learned.stats()["n_passes"]),
+               "same_plan": bool(same)}
         if i in unfused_set or i in check_set:
             CostModel.detach()
             t_un, p_un = plan_time_ms(c, "none")
@@ -265,11 +304,21 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     errs = [max(r["greedy_max_abs_vs_unfused"], r["learned_max_abs_vs_unfused"]) for r in rows
             if "greedy_max_abs_vs_unfused" in r]
     summary = {
+        "model": args.load or args.save,
         "train_circuits": len(train_spec), "eval_circuits": len(eval_spec), "train_rows": int(len(X)),
         "measure_s": t_measure, "train_s": t_train, "loss_initial": loss0, "loss_final": loss,
         "train_rmse_log_us": train_rmse,
         "eval_total_greedy_ms": float(gt.sum()), "eval_total_learned_ms": float(lt.sum()),
         "eval_learned_over_greedy": float(lt.sum() / gt.sum()),
+        "eval_learned_over_greedy_geomean": float(np.exp(np.mean(np.log(lt / gt)))),
+        "eval_same_plan_count": int(sum(r["same_plan"] for r in rows)),
+        "eval_differing_plans": int(sum(not r["same_plan"] for r in rows)),
+        "eval_differing_learned_over_greedy": (float(sum(r["learned_ms"] for r in rows if not r["same_plan"]) /
+                                                     sum(r["greedy_ms"] for r in rows if not r["same_plan"]))
+                                               if any(not r["same_plan"] for r in rows) else None),
+        "eval_same_plan_measured_ratio": (float(sum(r["learned_ms"] for r in rows if r["same_plan"]) /
+                                                sum(r["greedy_ms"] for r in rows if r["same_plan"]))
+                                          if any(r["same_plan"] for r in rows) else None),
         "eval_learned_faster_count": int((lt < gt * 0.995).sum()), "eval_learned_slower_count": int((lt > gt * 1.005).sum()),
         "unfused_subset": len(un), "unfused_total_ms": float(sum(u for u, _, _ in un)),
         "greedy_total_on_unfused_subset_ms": float(sum(g for _, g, _ in un)),

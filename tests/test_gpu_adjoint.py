@@ -214,3 +214,19 @@ def test_tiled_sweep_needs_a_full_tile():
     npar = int((pidx >= 0).sum())
     with pytest.raises(ValueError):
         adjoint_expval(circ, pidx, np.zeros((1, npar)), [(1.0, "Z" * 10)], "c64", method="tiled")
+
+
+def test_hamiltonian_with_more_terms_than_shared_memory_holds(oracle):
+    """1100 Pauli terms: lambda = H psi takes the global-memory form (the
+    shared-memory form holds 1024 terms)."""
+    from ket_b200.autograd import adjoint_expval
+    from ket_b200.workloads import random_pauli_sum, variational_ansatz
+    n = 12
+    circ, pidx = variational_ansatz(n, 2)
+    npar = int((pidx >= 0).sum())
+    ham = random_pauli_sum(n, 1100, seed=31)
+    theta = np.random.default_rng(32).uniform(-math.pi, math.pi, (1, npar))
+    vals, grads = adjoint_expval(circ, pidx, theta, ham, "c128", checkpoint_every=1)
+    v, g = oracle.adjoint(n, circ.to_ops(), pidx, theta[0], ham)
+    assert abs(vals[0] - v) < 1e-9
+    assert np.abs(grads[0] - g).max() < 1e-9

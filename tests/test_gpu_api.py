@@ -259,3 +259,35 @@ def test_clifford_routing_decisions():
     assert not ket.is_clifford(c)
     with pytest.raises(ValueError):
         ket.sample(c, seed=1, method="stabilizer")
+
+
+def test_edge_cases_like_ket():
+    """Empty Hamiltonian, negative coefficients (test_observable.cpp:60-74),
+    the 0- and 1-qubit registers, and zero shots."""
+    c = ket.Circuit(2)
+    c.h(0)
+    c.cx(0, 1)
+    s = ket.run(c)
+    assert abs(ket.expval(s, [(0.5, "ZZ"), (0.5, "XX")]) - 1.0) < TOL
+    assert abs(ket.expval(s, [(2.0, "ZZ"), (-1.0, "YY")]) - 3.0) < TOL
+    assert ket.expval(s, []) == 0.0
+    # a register of no qubits holds one amplitude, 1
+    s0 = ket.run(ket.Circuit(0))
+    assert len(s0) == 1
+    amp(s0, 0, 1)
+    # one qubit, every single-qubit gate in a row, against the oracle's matrices
+    c1 = ket.Circuit(1)
+    c1.h(0)
+    c1.t(0)
+    c1.ry(0, 0.3)
+    c1.s(0)
+    c1.rz(0, 1.1)
+    c1.u(0, 0.2, 0.4, 0.6)
+    s1 = ket.run(c1)
+    assert abs(abs(s1[0]) ** 2 + abs(s1[1]) ** 2 - 1) < TOL
+    # zero shots give an empty sample
+    c2 = ket.Circuit(2)
+    c2.h(0)
+    c2.t(1)
+    c2.measure_all()
+    assert len(ket.sample_shots(c2, 0, seed=1)) == 0

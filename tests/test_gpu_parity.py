@@ -267,3 +267,30 @@ def test_diagonal_heavy_random(oracle, n, seed):
         got = gpu_run(n, ops, "c64", "greedy", 5, tc)
         assert np.abs(got - want).max() < TOL32
         assert fidelity(got, want) > 1 - FID32
+
+
+@pytest.mark.parametrize("qs", [[0, 1], [3, 9], [1, 2, 3], [0, 7, 12]])
+def test_small_blocks_padded_onto_the_tensor_cores(oracle, qs):
+    """2- and 3-qubit dense blocks in complex64 run as 4-qubit tensor-core
+    blocks (identity on the padding qubits)."""
+    import ket_b200 as kb
+    from ket_b200 import _lib
+    n = 14
+    prep = _block_circuit(n, list(range(n)), seed=5, depth=2 * n)
+    blk = _block_circuit(n, qs, seed=17)
+    ops = np.concatenate([prep, blk])
+    want = oracle.run(n, ops, fuse=0)
+    got = gpu_run(n, ops, "c64", "greedy", len(qs), True)
+    assert np.abs(got - want).max() < TOL32
+    assert fidelity(got, want) > 1 - FID32
+    opt = kb.make_options("c64", "greedy", len(qs), True)
+    h = ct.c_void_p()
+    _lib.check(_lib.lib.ketgpu_plan_create(n, blk.ctypes.data, len(blk), ct.byref(opt), ct.byref(h)))
+    ks = []
+    for i in range(int(kb.plan_stats(type("C", (), {"to_ops": lambda s: blk, "n_qubits": n})(), opt)["n_passes"])):
+        kind, k, tc, b = ct.c_int32(), ct.c_int32(), ct.c_int32(), ct.c_double()
+        _lib.check(_lib.lib.ketgpu_plan_pass_info(h, i, ct.byref(kind), ct.byref(k), ct.byref(tc), ct.byref(b)))
+        if kind.value == 2:
+            ks.append((k.value, tc.value))
+    _lib.lib.ketgpu_plan_destroy(h)
+    assert ks and all(x == (4, 1) for x in ks)
