@@ -441,6 +441,16 @@ class Plan:
         check(lib.ketgpu_plan_stats_get(self._h, ct.byref(st)))
         return {f: getattr(st, f) for f, _ in _lib.PlanStats._fields_}
 
+    def pass_info(self, index: int) -> dict:
+        """Kind (0 pair, 1 phase, 2 dense block, 3 norm, 4 diagonal run),
+        qubits k, tensor-core flag and algorithmic HBM bytes of one pass."""
+        kind, k, tc, b = ct.c_int32(), ct.c_int32(), ct.c_int32(), ct.c_double()
+        check(lib.ketgpu_plan_pass_info(self._h, index, ct.byref(kind), ct.byref(k), ct.byref(tc), ct.byref(b)))
+        return {"kind": kind.value, "k": k.value, "tensor": bool(tc.value), "bytes": b.value}
+
+    def pass_bytes(self, index: int) -> float:
+        return self.pass_info(index)["bytes"]
+
     def execute(self, state: DeviceState, sync: bool = True):
         check(lib.ketgpu_plan_execute(self._h, state.handle))
         if sync:

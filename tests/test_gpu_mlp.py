@@ -63,3 +63,60 @@ def test_learned_plans_are_correct(oracle):
     finally:
         CostModel.detach()
         m.close()
+
+
+def test_trained_network_predicts_pass_times_better_than_the_static_model():
+    """What the trained cost model adds over the planner without it: on
+    held-out corpus circuits, the network's pass-time predictions beat the
+    static model (time proportional to the bytes a pass moves, its one scale
+    fitted to these very passes), and on the held-out circuits where the
+    learned plan differs from greedy it is no slower."""
+    import ket_b200 as ket
+    from ket_b200 import planner as pl
+    from ket_b200.workloads import random_mixed
+    model = pl.CostModel.load()
+    rows_x, rows_y, rows_b = [], [], []
+    for n, d, s in [(22, 30, 11), (23, 40, 12), (24, 25, 13), (25, 35, 14)]:
+        c = random_mixed(n, d, seed=s)
+        for fusion, k in (("none", 5), ("greedy", 3), ("greedy", 5)):
+            plan = ket.Plan(n, c.to_ops(), ket.make_options("c64", fusion, k, True))
+            ms = pl.timed_execute(plan, pl._state(n))
+            for rep in range(2):  # best of three per pass
+                ms = np.minimum(ms, pl.timed_execute(plan, pl._state(n)))
+            for i in range(len(ms)):
+                rows_x.append(pl.pass_features(plan, i))
+                rows_y.append(np.log(max(float(ms[i]) * 1e3, 1e-3)))
+                rows_b.append(plan.pass_bytes(i))
+            plan.close()
+    x = np.array(rows_x, dtype=np.float32)
+    y = np.array(rows_y)
+    b = np.array(rows_b)
+    net = model.forward(x).astype(np.float64)
+    # static model: log t = log(bytes) + log(scale), the scale fitted here
+    static = np.log(b) + np.mean(y - np.log(b))
+    rmse_net = float(np.sqrt(np.mean((net - y) ** 2)))
+    rmse_static = float(np.sqrt(np.mean((static - y) ** 2)))
+    print(f"pass-time log-RMSE: network {rmse_net:.3f}, static {rmse_static:.3f} over {len(y)} passes")
+    assert rmse_net < rmse_static
+    # held-out circuits whose learned plan differs from greedy (planner_eval.json)
+    import json
+    import os
+    rows = json.load(open(os.path.join(os.path.dirname(pl.__file__), "data", "planner_eval.json")))["rows"]
+    diff = [r for r in rows if not r["same_plan"] and r["n"] <= 26]
+    tg = tl = 0.0
+    for r in diff:
+        c = random_mixed(r["n"], r["depth"], seed=r["seed"])
+        pl.CostModel.detach()
+        pg = ket.Plan(r["n"], c.to_ops(), ket.make_options("c64", "greedy", 5, True))
+        model.attach()
+        plr = ket.Plan(r["n"], c.to_ops(), ket.make_options("c64", "learned", 5, True))
+        pl.CostModel.detach()
+        st = pl._state(r["n"])
+        g = min(float(pl.timed_execute(pg, st).sum()) for _ in range(3))
+        l_ = min(float(pl.timed_execute(plr, st).sum()) for _ in range(3))
+        tg, tl = tg + g, tl + l_
+        pg.close()
+        plr.close()
+    if diff:
+        print(f"learned / greedy on {len(diff)} differing held-out circuits: {tl / tg:.4f}")
+        assert tl <= 1.02 * tg
