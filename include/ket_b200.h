@@ -214,6 +214,11 @@ int ketgpu_adjoint(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
 #define KETGPU_ADJOINT_AUTO 0
 #define KETGPU_ADJOINT_PER_GATE 1
 #define KETGPU_ADJOINT_TILED 2
+/* TILED with each complex64 block's kernel generated with its gates as
+ * compile-time constants and compiled at run time (NVRTC, cached per process
+ * by block structure; AUTO chooses it for complex64 from 16 qubits).  Falls
+ * back to TILED when NVRTC is unavailable. */
+#define KETGPU_ADJOINT_TILED_JIT 3
 int ketgpu_adjoint_ex(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
                       const int32_t* param_index, const double* params,
                       uint64_t n_params, uint64_t batch, const double* coeffs,
@@ -223,6 +228,9 @@ int ketgpu_adjoint_ex(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
 /* The tiled sweeps' plan as flat int32 records (layout documented in
  * ket_b200/csrc/adjoint.cu); *length receives the record count, out may be
  * NULL to query it. */
+/* NVRTC availability, distinct per-block kernels compiled so far, and
+ * launches that used one. */
+int ketgpu_adjoint_jit_info(int32_t* available, uint64_t* kernels, uint64_t* launches);
 int ketgpu_adjoint_plan_describe(int32_t n_qubits, const ketgpu_op* ops,
                                  uint64_t n_ops, const int32_t* param_index,
                                  int32_t precision, int32_t* out,

@@ -25,8 +25,8 @@ def adjoint_expval(circuit: Circuit, param_index: np.ndarray, params: np.ndarray
                    checkpoint_every: int = 2, method: str = "auto") -> Tuple[np.ndarray, np.ndarray]:
     """values (batch,), grads (batch, n_params) for params of shape (batch, n_params).
 
-    method: "auto", "per_gate" or "tiled" (the sweep kernels; same results up
-    to rounding)."""
+    method: "auto", "per_gate", "tiled" or "tiled_jit" (the sweep kernels;
+    same results up to rounding)."""
     ops = circuit.to_ops()
     pidx = np.ascontiguousarray(param_index, dtype=np.int32)
     if len(pidx) != len(ops):
@@ -38,11 +38,21 @@ def adjoint_expval(circuit: Circuit, param_index: np.ndarray, params: np.ndarray
     values = np.zeros(batch, dtype=np.float64)
     grads = np.zeros((batch, npar), dtype=np.float64)
     prec = {"c64": _lib.C64, "c128": _lib.C128}[precision]
-    meth = {"auto": 0, "per_gate": 1, "tiled": 2}[method]
+    meth = {"auto": 0, "per_gate": 1, "tiled": 2, "tiled_jit": 3}[method]
     check(lib.ketgpu_adjoint_ex(circuit.n_qubits, ops.ctypes.data, len(ops), pidx.ctypes.data, prm.ctypes.data,
                                 npar, batch, coeffs.ctypes.data, ct.cast(arr, ct.c_void_p), len(hamiltonian),
                                 prec, int(checkpoint_every), meth, values.ctypes.data, grads.ctypes.data))
     return values, grads
+
+
+def jit_info() -> dict:
+    """Per-block compiled adjoint kernels: NVRTC availability, kernels cached
+    and launches so far."""
+    a = ct.c_int32()
+    k = ct.c_uint64()
+    n = ct.c_uint64()
+    check(lib.ketgpu_adjoint_jit_info(ct.byref(a), ct.byref(k), ct.byref(n)))
+    return {"available": bool(a.value), "kernels": k.value, "launches": n.value}
 
 
 def _function():

@@ -24,13 +24,14 @@ CXX = os.environ.get("CXX", "g++")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++20", "-Xcompiler", "-fPIC,-fvisibility=hidden",
-                  "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
+                  "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"), "-I" + OBJ]
 CXXFLAGS = ["-O2", "-std=c++20", "-fPIC", "-fvisibility=hidden", "-Wall", "-Wextra",
             "-I" + os.path.join(CUDA, "include"), "-I" + os.path.join(ROOT, "include")]
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+            glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
 def _stale(src, obj, deps):
@@ -51,9 +52,23 @@ def _run(cmd, verbose):
         sys.stderr.write(r.stdout + r.stderr)
 
 
+def _embed_tile_source():
+    """adj_tile.cuh as a C++ string literal (the per-block adjoint kernels are
+    compiled from it at run time)."""
+    src = os.path.join(CSRC, "adj_tile.cuh")
+    out = os.path.join(OBJ, "adj_tile_src.inc")
+    if os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src):
+        return out
+    text = open(src).read()
+    assert ')KBSRC"' not in text
+    with open(out, "w") as f:
+        f.write('R"KBSRC(' + text + ')KBSRC"\n')
+    return out
+
+
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    deps = _headers()
+    deps = _headers() + [_embed_tile_source()]
     objs, jobs = [], []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")
@@ -88,7 +103,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         raise RuntimeError("ket_b200: compilation failed")
     if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs +
-             ["-Xcompiler", "-fPIC", "-Xlinker", "--no-undefined", "-lpthread"], verbose)
+             ["-Xcompiler", "-fPIC", "-Xlinker", "--no-undefined", "-lpthread", "-ldl"], verbose)
     return LIB
 
 

@@ -18,8 +18,12 @@
 // is stored every m layers and the reverse sweep restarts psi from it, so
 // the uncomputation error does not accumulate across segments.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -29,6 +33,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "adj_tile.cuh"
 
 #define KB_API extern "C" __attribute__((visibility("default")))
 
@@ -330,61 +335,10 @@ __global__ void ground_batch(typename C2T<R>::T* states, uint64_t dim) {
 // the warp in FP64 and accumulated per warp and gate in shared memory (FP64),
 // then summed in fixed order over warps, CTAs and (on the host) blocks.
 
-template <typename R>
-struct TileCfg;
-template <>
-struct TileCfg<float> {
-  static constexpr int TB = 12, RB = 4;
-};
-template <>
-struct TileCfg<double> {
-  static constexpr int TB = 11, RB = 3;
-};
-constexpr int kTileThreads = 256;  // 2^(TB - RB) in both precisions
-constexpr int kTileWarps = kTileThreads / 32;
-constexpr int kMaxBlockGrads = 64;
-constexpr int kMaxBlockGates = 256;
-
-enum TKind : uint8_t { kTPair = 0, kTPairSwap = 1, kTSwap2 = 2, kTDiag = 3 };
-
-struct TGate {
-  uint8_t kind;
-  uint8_t s0, s1;  // register slots of the target(s) (pair kinds; s0 < s1 for kTSwap2)
-  int8_t tslot;    // kTDiag: register slot of the target bit, or -1
-  uint8_t tbit;    // kTDiag: tile bit of the target
-  uint8_t cm_r;    // controls held in registers, as a register-index mask
-  uint8_t gen;     // gradient generator: 0 none, 1 X, 2 Y, 3 Z, 4 P11
-  uint8_t real;    // kTPair: the matrix is real for every parameter set
-  uint16_t cm_g;   // controls not held in registers, as a tile-bit mask
-  int16_t grad;    // gradient slot within the block, or -1
-  int32_t mat;     // gate index into the per-set matrix table
-};
-static_assert(sizeof(TGate) == 16, "TGate layout");
-
-struct TPhase {
-  uint8_t r[4];  // tile bits held in registers (register-index bit b <-> r[b])
-  int32_t first, count;  // gates of the phase, relative to the block's first gate
-};
-
-struct TileGeom {
-  uint64_t n_tiles;
-  int pos[12];  // tile bit -> qubit, ascending; pos[0..4] = 0..4
-};
-
-// Shared-memory swizzle: XOR-folds the higher bit groups into the lowest so
-// that a half-warp (8-byte elements) or quarter-warp (16-byte elements)
-// touching 16 (8) elements that differ in any four (three) tile bits hits
-// distinct banks in the common layouts.
-template <typename R>
-__device__ __forceinline__ int tphys(int e);
-template <>
-__device__ __forceinline__ int tphys<float>(int e) {
-  return e ^ (((e >> 4) ^ (e >> 8)) & 15);
-}
-template <>
-__device__ __forceinline__ int tphys<double>(int e) {
-  return e ^ (((e >> 3) ^ (e >> 6) ^ (e >> 9)) & 7);
-}
+// TileCfg, TGate, TPhase, TileGeom, the swizzle, the asynchronous copy and
+// the packed complex64 gate code live in adj_tile.cuh, shared with the
+// per-block kernels compiled at run time.
+using namespace kbt;
 
 template <typename R>
 struct CM2 {
@@ -594,15 +548,6 @@ __device__ __forceinline__ R tile_gate(typename C2T<R>::T* p, typename C2T<R>::T
                 : tile_gate_rc<R, RB, REV, false>(p, q, g, m, gbase);
 }
 
-// Asynchronous global -> shared copy of one amplitude (8 or 16 bytes).
-__device__ __forceinline__ void tile_cp_async(float2* dst, const float2* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void tile_cp_async(double2* dst, const double2* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
 
 // Forward (REV = false: psi only, gates in order) or reverse (REV = true:
 // psi and lambda, gates in reverse order, gradient partials) over one block,
@@ -769,242 +714,6 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     }
 }
 
-// ---------------------------------------------------------------------------
-// complex64 tiled sweeps on packed pairs.  Blackwell's f32x2 instructions
-// (fma.rn.f32x2, mul.rn.f32x2) do two FP32 operations each.  Register slot 0 of a
-// complex64 phase is its pack bit: no gate of the phase targets it with a
-// pair or uses it as a control (the planner guarantees it), so the two
-// amplitudes that differ only in that bit always meet the same coefficients
-// and live in one 64-bit register pair: re = (re_lo, re_hi), im = (im_lo,
-// im_hi).  A thread's 16 amplitudes of a state are 8 such packs of each
-// part; a gate on register slot S (1..3) acts across packs jo and
-// jo | 1 << (S-1).  A diagonal gate may target the pack bit itself (its two
-// phases then form a per-half pack).  Per gate the shared memory holds 16
-// packed coefficients of U (forward) or U^dag (reverse):
-//   [0..7]  c0r c0i c1r c1i c2r c2i c3r c3i, each duplicated in both halves
-//   [8..11] -c0i -c1i -c2i -c3i
-//   [12..14] (c0r, c3r) (c0i, c3i) (-c0i, -c3i): a diagonal on the pack bit
-using f2 = unsigned long long;  // (lo, hi) halves in one 64-bit register pair
-
-__device__ __forceinline__ f2 pk2(float lo, float hi) {
-  f2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void upk2(f2 v, float& lo, float& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
-  f2 d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-__device__ __forceinline__ f2 mul2p(f2 a, f2 b) {
-  f2 d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ float hsum2(f2 v) {
-  float lo, hi;
-  upk2(v, lo, hi);
-  return lo + hi;
-}
-
-struct PackState {
-  f2 r[8], i[8];
-};
-
-// (xr, xi) <- complex phase (pr, pi) times (xr, xi); npi = -pi.
-__device__ __forceinline__ void pk_phase(f2& xr, f2& xi, f2 pr, f2 pi, f2 npi) {
-  const f2 nr = fma2(pr, xr, mul2p(npi, xi));
-  xi = fma2(pr, xi, mul2p(pi, xr));
-  xr = nr;
-}
-
-// 2x2 on packs a, b: (a, b) <- (c0 a + c1 b, c2 a + c3 b).
-template <bool REAL>
-__device__ __forceinline__ void pk_2x2(f2& ar, f2& ai, f2& br, f2& bi, const f2* c) {
-  if (REAL) {
-    const f2 xr = fma2(c[0], ar, mul2p(c[2], br)), xi = fma2(c[0], ai, mul2p(c[2], bi));
-    const f2 yr = fma2(c[4], ar, mul2p(c[6], br)), yi = fma2(c[4], ai, mul2p(c[6], bi));
-    ar = xr, ai = xi, br = yr, bi = yi;
-  } else {
-    const f2 xr = fma2(c[0], ar, fma2(c[8], ai, fma2(c[2], br, mul2p(c[9], bi))));
-    const f2 xi = fma2(c[0], ai, fma2(c[1], ar, fma2(c[2], bi, mul2p(c[3], br))));
-    const f2 yr = fma2(c[4], ar, fma2(c[10], ai, fma2(c[6], br, mul2p(c[11], bi))));
-    const f2 yi = fma2(c[4], ai, fma2(c[5], ar, fma2(c[6], bi, mul2p(c[7], br))));
-    ar = xr, ai = xi, br = yr, bi = yi;
-  }
-}
-
-// Gate bodies, fully specialised at compile time: register slot(s), real or
-// complex matrix, gradient generator (reverse only) and whether some
-// controls are register bits (RC; then each pack is tested against them).
-
-// Swap on outer slot S (1..3): X, CX, CCX.
-template <int S, bool REV, bool RC>
-__device__ __forceinline__ float pk_swap(PackState& a, PackState& l, const TGate& g) {
-  constexpr int so = S - 1;
-  const int cm = g.cm_r >> 1;
-#pragma unroll
-  for (int jo = 0; jo < 8; ++jo) {
-    if (jo & (1 << so)) continue;
-    if (RC && (jo & cm) != cm) continue;
-    const int j1 = jo | (1 << so);
-    f2 t = a.r[jo]; a.r[jo] = a.r[j1]; a.r[j1] = t;
-    t = a.i[jo]; a.i[jo] = a.i[j1]; a.i[j1] = t;
-    if (REV) {
-      t = l.r[jo]; l.r[jo] = l.r[j1]; l.r[j1] = t;
-      t = l.i[jo]; l.i[jo] = l.i[j1]; l.i[j1] = t;
-    }
-  }
-  return 0.f;
-}
-
-// 2x2 on outer slot S.  Reverse: the gradient term Im <l|G|a> first (GEN
-// 1 X, 2 Y, 3 Z), as plus and minus packed sums.
-template <int S, bool REAL, int GEN, bool REV, bool RC>
-__device__ __forceinline__ float pk_pair(PackState& a, PackState& l, const TGate& g, const f2* c) {
-  constexpr int so = S - 1;
-  const int cm = g.cm_r >> 1;
-  f2 plus = 0, minus = 0;
-#pragma unroll
-  for (int jo = 0; jo < 8; ++jo) {
-    if (jo & (1 << so)) continue;
-    if (RC && (jo & cm) != cm) continue;
-    const int j1 = jo | (1 << so);
-    if (REV && GEN == 1) {  // X: (l0r a1i - l0i a1r) + (l1r a0i - l1i a0r)
-      plus = fma2(l.r[jo], a.i[j1], fma2(l.r[j1], a.i[jo], plus));
-      minus = fma2(l.i[jo], a.r[j1], fma2(l.i[j1], a.r[jo], minus));
-    } else if (REV && GEN == 2) {  // Y: (l1r a0r + l1i a0i) - (l0r a1r + l0i a1i)
-      plus = fma2(l.r[j1], a.r[jo], fma2(l.i[j1], a.i[jo], plus));
-      minus = fma2(l.r[jo], a.r[j1], fma2(l.i[jo], a.i[j1], minus));
-    } else if (REV && GEN == 3) {  // Z: (l0r a0i - l0i a0r) - (l1r a1i - l1i a1r)
-      plus = fma2(l.r[jo], a.i[jo], fma2(l.i[j1], a.r[j1], plus));
-      minus = fma2(l.i[jo], a.r[jo], fma2(l.r[j1], a.i[j1], minus));
-    }
-    pk_2x2<REAL>(a.r[jo], a.i[jo], a.r[j1], a.i[j1], c);
-    if (REV) pk_2x2<REAL>(l.r[jo], l.i[jo], l.r[j1], l.i[j1], c);
-  }
-  return (REV && GEN) ? hsum2(plus) - hsum2(minus) : 0.f;
-}
-
-template <int A, int B, bool REV, bool RC>
-__device__ __forceinline__ float pk_swap2(PackState& a, PackState& l, const TGate& g) {
-  constexpr int oa = A - 1, ob = B - 1;
-  const int cm = g.cm_r >> 1;
-#pragma unroll
-  for (int jo = 0; jo < 8; ++jo) {
-    if (!(jo & (1 << oa)) || (jo & (1 << ob))) continue;
-    if (RC && (jo & cm) != cm) continue;
-    const int j1 = jo ^ (1 << oa) ^ (1 << ob);
-    f2 t = a.r[jo]; a.r[jo] = a.r[j1]; a.r[j1] = t;
-    t = a.i[jo]; a.i[jo] = a.i[j1]; a.i[j1] = t;
-    if (REV) {
-      t = l.r[jo]; l.r[jo] = l.r[j1]; l.r[j1] = t;
-      t = l.i[jo]; l.i[jo] = l.i[j1]; l.i[j1] = t;
-    }
-  }
-  return 0.f;
-}
-
-// Diagonal gate.  TS: register slot of the target (1..3), 0 for the pack
-// bit, -1 for a group bit (its value for this thread is read from gbase).
-// Gradient (GEN 3 Z, 4 P11): Im(conj(l) a) per amplitude, weighted +-1 by the
-// target bit (Z) or kept only where it is 1 (P11).
-template <int TS, int GEN, bool REV, bool RC>
-__device__ __forceinline__ float pk_diag(PackState& a, PackState& l, const TGate& g, const f2* c, int gbase) {
-  const int cm = g.cm_r >> 1;
-  const bool gbit = TS < 0 ? ((gbase >> g.tbit) & 1) : false;
-  f2 plus0 = 0, minus0 = 0, plus1 = 0, minus1 = 0;  // target bit 0 / 1
-  f2 pr0 = c[0], pi0 = c[1], npi0 = c[8], pr1 = c[6], pi1 = c[7], npi1 = c[11];
-  if (TS == 0) pr0 = c[12], pi0 = c[13], npi0 = c[14];
-  if (TS < 0 && gbit) pr0 = pr1, pi0 = pi1, npi0 = npi1;
-#pragma unroll
-  for (int jo = 0; jo < 8; ++jo) {
-    if (RC && (jo & cm) != cm) continue;
-    const bool bit = TS > 0 ? ((jo >> (TS - 1)) & 1) : false;  // compile time
-    const f2 pr = bit ? pr1 : pr0, pi = bit ? pi1 : pi0, npi = bit ? npi1 : npi0;
-    if (REV && GEN) {
-      if (!bit) {
-        plus0 = fma2(l.r[jo], a.i[jo], plus0);
-        minus0 = fma2(l.i[jo], a.r[jo], minus0);
-      } else {
-        plus1 = fma2(l.r[jo], a.i[jo], plus1);
-        minus1 = fma2(l.i[jo], a.r[jo], minus1);
-      }
-    }
-    pk_phase(a.r[jo], a.i[jo], pr, pi, npi);
-    if (REV) pk_phase(l.r[jo], l.i[jo], pr, pi, npi);
-  }
-  if (!(REV && GEN)) return 0.f;
-  float s0, s1;
-  if (TS == 0) {  // halves: lo = target bit 0, hi = target bit 1
-    float p0, p1, m0, m1;
-    upk2(plus0, p0, p1);
-    upk2(minus0, m0, m1);
-    s0 = p0 - m0;
-    s1 = p1 - m1;
-  } else if (TS < 0) {  // every element of the thread has target bit gbit
-    const float t = hsum2(plus0) - hsum2(minus0);
-    s0 = gbit ? 0.f : t;
-    s1 = gbit ? t : 0.f;
-  } else {
-    s0 = hsum2(plus0) - hsum2(minus0);
-    s1 = hsum2(plus1) - hsum2(minus1);
-  }
-  return GEN == 3 ? s0 - s1 : s1;
-}
-
-// Flat opcode of a gate, computed once per CTA when the block's gates are
-// staged (the generator counts only in the reverse sweep):
-//   pair   (S-1)*16 + real*8 + gen*2 + rc           0..47
-//   swap   48 + (S-1)*2 + rc                         48..53
-//   swap2  54 + {(1,2):0, (1,3):1, (2,3):2}*2 + rc   54..59
-//   diag   60 + (TS+1)*6 + {0:0, 3:1, 4:2}[gen]*2 + rc   60..89
-__device__ __forceinline__ int pk_opcode(const TGate& g, bool rev) {
-  const int rc = g.cm_r ? 1 : 0;
-  const int gen = rev ? g.gen : 0;
-  switch (g.kind) {
-    case kTPair: return (g.s0 - 1) * 16 + (g.real ? 8 : 0) + gen * 2 + rc;
-    case kTPairSwap: return 48 + (g.s0 - 1) * 2 + rc;
-    case kTSwap2: return 54 + (g.s0 == 1 ? (g.s1 == 2 ? 0 : 1) : 2) * 2 + rc;
-    default: return 60 + (g.tslot + 1) * 6 + (gen == 3 ? 1 : gen == 4 ? 2 : 0) * 2 + rc;
-  }
-}
-
-template <int OP, bool REV>
-__device__ __forceinline__ float pk_exec(PackState& a, PackState& l, const TGate& g, const f2* c, int gbase) {
-  if constexpr (OP < 48) {
-    return pk_pair<OP / 16 + 1, ((OP / 8) & 1) != 0, (OP / 2) & 3, REV, (OP & 1) != 0>(a, l, g, c);
-  } else if constexpr (OP < 54) {
-    return pk_swap<(OP - 48) / 2 + 1, REV, (OP & 1) != 0>(a, l, g);
-  } else if constexpr (OP < 60) {
-    constexpr int w = (OP - 54) / 2;
-    return pk_swap2<w == 2 ? 2 : 1, w == 0 ? 2 : 3, REV, (OP & 1) != 0>(a, l, g);
-  } else {
-    constexpr int t = (OP - 60) / 6, gi = ((OP - 60) % 6) / 2;
-    return pk_diag<t - 1, gi == 0 ? 0 : gi == 1 ? 3 : 4, REV, (OP & 1) != 0>(a, l, g, c, gbase);
-  }
-}
-
-#define KB_PK_CASE(N) \
-  case N: return pk_exec<N, REV>(a, l, g, c, gbase);
-#define KB_PK_CASE10(N)                                                                                    \
-  KB_PK_CASE(N + 0) KB_PK_CASE(N + 1) KB_PK_CASE(N + 2) KB_PK_CASE(N + 3) KB_PK_CASE(N + 4) KB_PK_CASE(N + 5) \
-  KB_PK_CASE(N + 6) KB_PK_CASE(N + 7) KB_PK_CASE(N + 8) KB_PK_CASE(N + 9)
-
-template <bool REV>
-__device__ __forceinline__ float pk_dispatch(int op, PackState& a, PackState& l, const TGate& g, const f2* c,
-                                             int gbase) {
-  switch (op) {
-    KB_PK_CASE10(0) KB_PK_CASE10(10) KB_PK_CASE10(20) KB_PK_CASE10(30) KB_PK_CASE10(40)
-    KB_PK_CASE10(50) KB_PK_CASE10(60) KB_PK_CASE10(70) KB_PK_CASE10(80)
-    default: return 0.f;
-  }
-}
-#undef KB_PK_CASE10
-#undef KB_PK_CASE
 
 // The complex64 form of tile_sweep (same grid, pipeline and partials).
 template <bool REV>
@@ -1472,6 +1181,199 @@ int gen_of(int type) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Per-block complex64 kernels compiled at run time.  The compiled sweep
+// (tile_sweep_c64) interprets each block's gate records: every gate goes
+// through a switch, and the register moves at its merge points dominate the
+// instruction count.  Here the block's phases and gates become compile-time
+// constants of a kernel generated from adj_tile.cuh: a swap is a renaming,
+// each gate is straight-line packed arithmetic.  The kernels are compiled
+// with NVRTC for sm_100a (loaded with dlopen on first use), loaded with the
+// runtime's library API and cached by their source text, so a layer
+// structure that repeats is compiled once per process.  When NVRTC cannot
+// be loaded or a compile fails, the compiled sweep runs instead.
+
+const char* const kTileSource =
+#include "adj_tile_src.inc"
+    ;
+
+struct Nvrtc {
+  using Create = int (*)(void**, const char*, const char*, int, const char* const*, const char* const*);
+  using Compile = int (*)(void*, int, const char* const*);
+  using SizeOf = int (*)(void*, size_t*);
+  using Get = int (*)(void*, char*);
+  using Destroy = int (*)(void**);
+  Create create = nullptr;
+  Compile compile = nullptr;
+  SizeOf log_size = nullptr, cubin_size = nullptr;
+  Get log = nullptr, cubin = nullptr;
+  Destroy destroy = nullptr;
+  bool ok = false;
+  Nvrtc() {
+    const char* names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"};
+    void* h = nullptr;
+    for (const char* n : names)
+      if ((h = dlopen(n, RTLD_NOW | RTLD_LOCAL))) break;
+    if (!h) return;
+    create = reinterpret_cast<Create>(dlsym(h, "nvrtcCreateProgram"));
+    compile = reinterpret_cast<Compile>(dlsym(h, "nvrtcCompileProgram"));
+    log_size = reinterpret_cast<SizeOf>(dlsym(h, "nvrtcGetProgramLogSize"));
+    log = reinterpret_cast<Get>(dlsym(h, "nvrtcGetProgramLog"));
+    cubin_size = reinterpret_cast<SizeOf>(dlsym(h, "nvrtcGetCUBINSize"));
+    cubin = reinterpret_cast<Get>(dlsym(h, "nvrtcGetCUBIN"));
+    destroy = reinterpret_cast<Destroy>(dlsym(h, "nvrtcDestroyProgram"));
+    ok = create && compile && log_size && log && cubin_size && cubin && destroy;
+  }
+};
+
+Nvrtc& nvrtc() {
+  static Nvrtc n;
+  return n;
+}
+
+// AUTO uses the per-block kernels from this many qubits up.
+constexpr int kJitMinQubits = 16;
+
+std::mutex g_jit_mu;
+std::map<std::string, cudaKernel_t> g_jit;  // source -> kernel (nullptr: failed)
+std::string g_jit_last_log;
+
+// Compile (once) and return the kernel "kb_tile_jit" of `src`, or nullptr.
+cudaKernel_t jit_kernel(const std::string& src) {
+  std::lock_guard<std::mutex> lock(g_jit_mu);
+  auto it = g_jit.find(src);
+  if (it != g_jit.end()) return it->second;
+  cudaKernel_t k = nullptr;
+  Nvrtc& nv = nvrtc();
+  if (nv.ok) {
+    const std::string full = std::string("#define KB_JIT 1\n") + kTileSource + src;
+    void* prog = nullptr;
+    if (nv.create(&prog, full.c_str(), "kb_tile_jit.cu", 0, nullptr, nullptr) == 0) {
+      const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17"};
+      const int rc = nv.compile(prog, 2, opts);
+      size_t ls = 0;
+      nv.log_size(prog, &ls);
+      std::string lg(ls, '\0');
+      if (ls) nv.log(prog, &lg[0]);
+      g_jit_last_log = lg;
+      size_t cs = 0;
+      if (rc == 0 && nv.cubin_size(prog, &cs) == 0 && cs) {
+        std::vector<char> cubin(cs);
+        if (nv.cubin(prog, cubin.data()) == 0) {
+          cudaLibrary_t lib = nullptr;
+          if (cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) == cudaSuccess &&
+              cudaLibraryGetKernel(&k, lib, "kb_tile_jit") != cudaSuccess)
+            k = nullptr;
+        }
+      }
+      nv.destroy(&prog);
+    }
+  }
+  cudaGetLastError();  // a failed load leaves no sticky error behind
+  g_jit[src] = k;
+  return k;
+}
+
+int tphys_host(int e) { return e ^ (((e >> 4) ^ (e >> 8)) & 15); }
+
+int pk_opcode_host(const TGate& g, bool rev) {
+  const int rc = g.cm_r ? 1 : 0;
+  const int gen = rev ? g.gen : 0;
+  switch (g.kind) {
+    case kTPair: return (g.s0 - 1) * 16 + (g.real ? 8 : 0) + gen * 2 + rc;
+    case kTPairSwap: return 48 + (g.s0 - 1) * 2 + rc;
+    case kTSwap2: return 54 + (g.s0 == 1 ? (g.s1 == 2 ? 0 : 1) : 2) * 2 + rc;
+    default: return 60 + (g.tslot + 1) * 6 + (gen == 3 ? 1 : gen == 4 ? 2 : 0) * 2 + rc;
+  }
+}
+
+// The kernel of one complex64 block: phases (in sweep order) and their gates
+// as constants.  Parameters as tile_sweep_c64, without the phase table.
+std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGate>& gates, bool rev) {
+  std::string o;
+  auto line = [&](const std::string& x) { o += x + "\n"; };
+  line("extern \"C\" __global__ void __launch_bounds__(256, " + std::string(rev ? "1" : "2") + ")");
+  line("kb_tile_jit(float2* __restrict__ psi, float2* __restrict__ lam, uint64_t dim, kbt::TileGeom tg,");
+  line("            const kbt::TGate* __restrict__ gates, int ngates, const float* __restrict__ mats,");
+  line("            uint64_t mat_stride, int ngrad, double* __restrict__ partial) {");
+  line("  using namespace kbt;");
+  line(std::string("  constexpr bool REV = ") + (rev ? "true" : "false") + ";");
+  line("  constexpr int TILE = 1 << TileCfg<float>::TB, BUF = (REV ? 2 : 1) * TILE;");
+  line("  extern __shared__ __align__(16) unsigned char tsm[];");
+  line("  float2* bufs = reinterpret_cast<float2*>(tsm);");
+  line("  f2* spk = reinterpret_cast<f2*>(tsm + 2 * BUF * sizeof(float2));");
+  line("  double* acc = reinterpret_cast<double*>(spk + 16 * ngates);");
+  line("  __shared__ uint64_t off_lo[64], off_hi[64];");
+  line("  const int tid = threadIdx.x;");
+  line("  const int set = blockIdx.y;");
+  line("  float2* s = psi + (uint64_t)set * dim;");
+  line("  float2* l = REV ? lam + (uint64_t)set * dim : nullptr;");
+  line("  c64_setup<REV>(tg, gates, ngates, mats, mat_stride, set, ngrad, off_lo, off_hi, spk, acc);");
+  line("  __syncthreads();");
+  line("  int cur = 0;");
+  line("  if (blockIdx.x < tg.n_tiles) c64_prefetch<REV>(tg, off_lo, off_hi, blockIdx.x, bufs, s, l);");
+  line("  asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");");
+  line("  for (uint64_t t = blockIdx.x; t < tg.n_tiles; t += gridDim.x) {");
+  line("    float2* sp = bufs + cur * BUF;");
+  line("    float2* sl = sp + TILE;");
+  line("    if (t + gridDim.x < tg.n_tiles)");
+  line("      c64_prefetch<REV>(tg, off_lo, off_hi, t + gridDim.x, bufs + (cur ^ 1) * BUF, s, l);");
+  line("    asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");");
+  line("    asm volatile(\"cp.async.wait_group 1;\\n\" ::: \"memory\");");
+  line("    __syncthreads();");
+  constexpr int TB = TileCfg<float>::TB;
+  const int nph = (int)phases.size();
+  for (int k = 0; k < nph; ++k) {
+    const TPhase& P = phases[rev ? nph - 1 - k : k];
+    int rmask = 0;
+    for (int b = 0; b < 4; ++b) rmask |= 1 << P.r[b];
+    std::string gb = "0";
+    for (int b = 0, kk = 0; b < TB; ++b)
+      if (!((rmask >> b) & 1)) gb += " | (((tid >> " + std::to_string(kk++) + ") & 1) << " + std::to_string(b) + ")";
+    line("    {");
+    line("      const int gbase = " + gb + ";");
+    line("      const int pg = tphys<float>(gbase);");
+    line("      PackState A, L;");
+    std::string pb;
+    for (int b = 0; b < 4; ++b) pb += ", " + std::to_string(tphys_host(1 << P.r[b]));
+    line("      c64_load_phase<REV>(sp, sl, pg" + pb + ", A, L);");
+    for (int c = 0; c < P.count; ++c) {
+      const int gi = rev ? P.first + P.count - 1 - c : P.first + c;
+      const TGate& g = gates[gi];
+      const int op = pk_opcode_host(g, rev);
+      char buf[512];
+      std::snprintf(buf, sizeof buf,
+                    "      { constexpr TGate g{%d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d}; float part = 0.f;",
+                    (int)g.kind, (int)g.s0, (int)g.s1, (int)g.tslot, (int)g.tbit, (int)g.cm_r, (int)(rev ? g.gen : 0),
+                    (int)g.real, (int)g.cm_g, (int)g.grad, 0);  // mat: read from the gate table at set-up
+      line(buf);
+      const std::string call = "part = pk_exec<" + std::to_string(op) + ", REV>(A, L, g, spk + 16 * " +
+                               std::to_string(gi) + ", gbase);";
+      if (g.cm_g) line("        if ((gbase & " + std::to_string((int)g.cm_g) + ") == " + std::to_string((int)g.cm_g) +
+                       ") " + call);
+      else line("        " + call);
+      if (rev && g.grad >= 0) line("        c64_grad(acc, ngrad, " + std::to_string((int)g.grad) + ", part);");
+      line("        (void)part; }");
+    }
+    line("      c64_store_phase<REV>(sp, sl, pg" + pb + ", A, L);");
+    line("      __syncthreads();");
+    line("    }");
+  }
+  line("    c64_store_tile<REV>(tg, off_lo, off_hi, t, sp, sl, s, l);");
+  line("    __syncthreads();");
+  line("    cur ^= 1;");
+  line("  }");
+  line("  asm volatile(\"cp.async.wait_all;\\n\" ::: \"memory\");");
+  line("  if (REV) c64_flush(acc, ngrad, partial, set);");
+  line("}");
+  return o;
+}
+
+size_t jit_smem(bool rev, int ngates, int ngrad) {
+  return (rev ? 4 : 2) * (size_t{1} << TileCfg<float>::TB) * sizeof(float2) + (size_t)ngates * 16 * sizeof(f2) +
+         (rev ? (size_t)kTileWarps * ngrad * 8 : 0);
+}
+
 // Dynamic shared memory of one tiled sweep launch (see the kernels).
 template <typename R>
 size_t tile_smem(bool rev, int ngates, int ngrad) {
@@ -1481,11 +1383,33 @@ size_t tile_smem(bool rev, int ngates, int ngrad) {
   return tiles + (size_t)ngates * per_gate + (rev ? (size_t)kTileWarps * ngrad * 8 : 0);
 }
 
+std::atomic<uint64_t> g_jit_launches{0};
+
 template <typename R, bool REV>
 void launch_tile(dim3 grid, cudaStream_t st, typename C2T<R>::T* psi, typename C2T<R>::T* lam, uint64_t dim,
                  const TBlock& b, const TGate* gates, const TPhase* phases, const R* mats, uint64_t chunk,
-                 double* partial) {
+                 double* partial, cudaKernel_t jit = nullptr) {
   const int ngrad = REV ? (int)b.grad_gate.size() : 0;
+  if constexpr (sizeof(R) == 4) {
+    if (jit) {
+      float2* a0 = psi;
+      float2* a1 = lam;
+      uint64_t d = dim;
+      TileGeom tg = b.geom;
+      const TGate* gp = gates + b.gate_first;
+      int ng = b.n_gates;
+      const float* mp = mats;
+      uint64_t ms = chunk;
+      int ngr = ngrad;
+      double* pp = partial;
+      void* args[] = {&a0, &a1, &d, &tg, &gp, &ng, &mp, &ms, &ngr, &pp};
+      KB_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(jit), grid, dim3(kTileThreads), args,
+                               jit_smem(REV, b.n_gates, ngrad), st));
+      count_launch();
+      g_jit_launches.fetch_add(1, std::memory_order_relaxed);
+      return;
+    }
+  }
   const size_t smem = tile_smem<R>(REV, b.n_gates, ngrad);
   if constexpr (sizeof(R) == 4)
     tile_sweep_c64<REV><<<grid, kTileThreads, smem, st>>>(psi, lam, dim, b.geom, gates + b.gate_first, b.n_gates,
@@ -1507,7 +1431,12 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
   constexpr int TB = TileCfg<R>::TB;
   const uint64_t dim = uint64_t{1} << n;
   const int T_ = (int)flip.size();
-  const bool tiled = method == KETGPU_ADJOINT_TILED || (method == KETGPU_ADJOINT_AUTO && n >= TB);
+  const bool tiled = method == KETGPU_ADJOINT_TILED || method == KETGPU_ADJOINT_TILED_JIT ||
+                     (method == KETGPU_ADJOINT_AUTO && n >= TB);
+  // per-block compiled kernels: complex64, asked for, or chosen at sizes
+  // where the sweeps take long enough to repay a compile
+  const bool want_jit = sizeof(R) == 4 && tiled &&
+                        (method == KETGPU_ADJOINT_TILED_JIT || (method == KETGPU_ADJOINT_AUTO && n >= kJitMinQubits));
   if (tiled && n < TB)
     fail(KETGPU_ERR_INVALID, "adjoint: the tiled sweep needs at least " + std::to_string(TB) + " qubits");
   // gates (unitary ops) and layer boundaries (barriers)
@@ -1624,6 +1553,7 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
 
   // tiled plan
   TilePlan tp;
+  std::vector<cudaKernel_t> jit_fwd, jit_rev;
   std::unique_ptr<DevBuf> d_tgates, d_tphases;
   int gx = 1;
   size_t grad_doubles = 0;
@@ -1645,6 +1575,26 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
     if (!tp.phases.empty())
       KB_CUDA(cudaMemcpyAsync(d_tphases->p, tp.phases.data(), sizeof(TPhase) * tp.phases.size(),
                               cudaMemcpyHostToDevice, st));
+    if (want_jit && nvrtc().ok) {
+      jit_fwd.assign(tp.blocks.size(), nullptr);
+      jit_rev.assign(tp.blocks.size(), nullptr);
+      for (size_t bi = 0; bi < tp.blocks.size(); ++bi) {
+        const TBlock& b = tp.blocks[bi];
+        const std::vector<TPhase> ph(tp.phases.begin() + b.phase_first,
+                                     tp.phases.begin() + b.phase_first + b.n_phases);
+        const std::vector<TGate> gs(tp.gates.begin() + b.gate_first, tp.gates.begin() + b.gate_first + b.n_gates);
+        jit_fwd[bi] = jit_kernel(jit_source(ph, gs, false));
+        jit_rev[bi] = jit_kernel(jit_source(ph, gs, true));
+        if (jit_fwd[bi])
+          KB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(jit_fwd[bi]),
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)jit_smem(false, kMaxBlockGates, 0)));
+        if (jit_rev[bi])
+          KB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(jit_rev[bi]),
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)jit_smem(true, kMaxBlockGates, kMaxBlockGrads)));
+      }
+    }
     const uint64_t n_tiles = uint64_t{1} << (n - TB);
     // one CTA per SM: about 4 waves of 148 CTAs over the chunk's sets
     gx = (int)std::min<uint64_t>(n_tiles, std::max<uint64_t>(1, (148ull * 4 + chunk - 1) / chunk));
@@ -1700,7 +1650,8 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
         while (next_ck < n_ckpt && next_ck * m <= b.layer) store_ck();
         dim3 grid((unsigned)gx, (unsigned)nb);
         launch_tile<R, false>(grid, st, psi.as<T>(), nullptr, dim, b, d_tgates->as<TGate>(), d_tphases->as<TPhase>(),
-                              mats_t.as<R>(), chunk, nullptr);
+                              mats_t.as<R>(), chunk, nullptr,
+                              jit_fwd.empty() ? nullptr : jit_fwd[&b - tp.blocks.data()]);
       }
     } else {
       for (size_t gi = 0; gi < G; ++gi) {
@@ -1735,7 +1686,8 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
                                   cudaMemcpyDeviceToDevice, st));
         dim3 grid((unsigned)gx, (unsigned)nb);
         launch_tile<R, true>(grid, st, psi.as<T>(), lam.as<T>(), dim, b, d_tgates->as<TGate>(),
-                             d_tphases->as<TPhase>(), mats_t.as<R>(), chunk, part.as<double>() + b.part_off);
+                             d_tphases->as<TPhase>(), mats_t.as<R>(), chunk, part.as<double>() + b.part_off,
+                             jit_rev.empty() ? nullptr : jit_rev[bi]);
       }
     } else {
       for (size_t gi = G; gi-- > 0;) {
@@ -1802,7 +1754,7 @@ int adjoint_entry(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const int32_t
     if (n < 1 || n > 34) fail(KETGPU_ERR_INVALID, "adjoint: n_qubits must be in [1, 34]");
     if (!ops || !values || !grads || (n_params && !params) || !coeffs || !paulis || n_terms == 0)
       fail(KETGPU_ERR_INVALID, "adjoint: null argument");
-    if (method < KETGPU_ADJOINT_AUTO || method > KETGPU_ADJOINT_TILED) fail(KETGPU_ERR_INVALID, "adjoint: bad method");
+    if (method < KETGPU_ADJOINT_AUTO || method > KETGPU_ADJOINT_TILED_JIT) fail(KETGPU_ERR_INVALID, "adjoint: bad method");
     validate_ops(n, ops, n_ops);
     std::vector<uint64_t> flip(n_terms), sign(n_terms);
     std::vector<int> q(n_terms);
@@ -1909,6 +1861,25 @@ KB_API int ketgpu_adjoint_plan_describe(int32_t n, const ketgpu_op* ops, uint64_
   } catch (const Error& e) {
     kb::set_last_error(e.what());
     return e.code;
+  } catch (const std::exception& e) {
+    kb::set_last_error(e.what());
+    return KETGPU_ERR_LOGIC;
+  }
+}
+
+// Per-block compiled adjoint kernels: whether NVRTC could be loaded, how
+// many distinct kernels are cached and how many launches used one.
+KB_API int ketgpu_adjoint_jit_info(int32_t* available, uint64_t* kernels, uint64_t* launches) {
+  try {
+    if (available) *available = nvrtc().ok ? 1 : 0;
+    if (kernels) {
+      std::lock_guard<std::mutex> lock(g_jit_mu);
+      uint64_t c = 0;
+      for (const auto& kv : g_jit) c += kv.second != nullptr;
+      *kernels = c;
+    }
+    if (launches) *launches = g_jit_launches.load();
+    return KETGPU_OK;
   } catch (const std::exception& e) {
     kb::set_last_error(e.what());
     return KETGPU_ERR_LOGIC;
