@@ -242,9 +242,16 @@ __global__ void __launch_bounds__(kAThreads)
   }
 }
 
-// The same with the terms in shared memory, the phase i^q folded into a
-// complex coefficient, and eight gathers in flight per thread.  Terms:
-// flip, sign mask, coefficient (re, im); at most kHamSmemTerms.
+// lambda = H psi for states larger than L2, split by the top qubit.  A
+// Pauli term maps output half h to source half h ^ (flip's top bit), so the
+// terms are grouped by that bit and each output half is built in two passes:
+// first from the terms that read the same half, then (adding to lambda) from
+// those that read the other half.  Each pass gathers from one half (67 MB at
+// 24 qubits, complex64), which stays in L2 while the pass's terms revisit
+// it.  The grid (CTAs per set x sets) covers about one set at a time.  Terms
+// sit in shared memory with the phase i^q folded into a complex
+// coefficient; eight gathers are in flight per thread.  The last pass of a
+// half adds Re <psi|lambda> over it into per-CTA partials.
 constexpr int kHamSmemTerms = 1024;
 struct HamTerm {
   uint64_t flip, sign;
@@ -253,8 +260,8 @@ struct HamTerm {
 
 template <typename R>
 __global__ void __launch_bounds__(kAThreads)
-    ham_apply_smem(const typename C2T<R>::T* __restrict__ psi, typename C2T<R>::T* __restrict__ lam, uint64_t dim,
-                   const HamTerm* __restrict__ terms, int nterms, double* __restrict__ partial) {
+    ham_half(const typename C2T<R>::T* __restrict__ psi, typename C2T<R>::T* __restrict__ lam, uint64_t dim, int h,
+             int first, int last, const HamTerm* __restrict__ terms, int nterms, double* __restrict__ epart) {
   using T = typename C2T<R>::T;
   __shared__ double sh[32];
   extern __shared__ __align__(16) unsigned char hsm[];
@@ -263,10 +270,17 @@ __global__ void __launch_bounds__(kAThreads)
   __syncthreads();
   const T* s = psi + (uint64_t)blockIdx.y * dim;
   T* l = lam + (uint64_t)blockIdx.y * dim;
+  const uint64_t half = dim >> 1, lo = h ? half : 0, hi = h ? dim : half;
   double e = 0.0;
-  for (uint64_t y = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; y < dim;
+  for (uint64_t y = lo + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; y < hi;
        y += (uint64_t)gridDim.x * blockDim.x) {
     double re = 0.0, im = 0.0;
+    if (!first) {  // lambda and psi[y] stream through (evict-first) so the
+                   // gathered half keeps L2
+      const T p = __ldcs(l + y);
+      re = p.x;
+      im = p.y;
+    }
     int t = 0;
     for (; t + 8 <= nterms; t += 8) {
       T a[8];
@@ -274,30 +288,33 @@ __global__ void __launch_bounds__(kAThreads)
       for (int u = 0; u < 8; ++u) a[u] = s[y ^ st[t + u].flip];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
-        const HamTerm& h = st[t + u];
+        const HamTerm& hm = st[t + u];
         const double ar = a[u].x, ai = a[u].y;
-        const bool neg = __popcll((y ^ h.flip) & h.sign) & 1;
-        const double cr = neg ? -h.cr : h.cr, ci = neg ? -h.ci : h.ci;
+        const bool neg = __popcll((y ^ hm.flip) & hm.sign) & 1;
+        const double cr = neg ? -hm.cr : hm.cr, ci = neg ? -hm.ci : hm.ci;
         re += cr * ar - ci * ai;
         im += cr * ai + ci * ar;
       }
     }
     for (; t < nterms; ++t) {
-      const HamTerm& h = st[t];
-      const T a = s[y ^ h.flip];
+      const HamTerm& hm = st[t];
+      const T a = s[y ^ hm.flip];
       const double ar = a.x, ai = a.y;
-      const bool neg = __popcll((y ^ h.flip) & h.sign) & 1;
-      const double cr = neg ? -h.cr : h.cr, ci = neg ? -h.ci : h.ci;
+      const bool neg = __popcll((y ^ hm.flip) & hm.sign) & 1;
+      const double cr = neg ? -hm.cr : hm.cr, ci = neg ? -hm.ci : hm.ci;
       re += cr * ar - ci * ai;
       im += cr * ai + ci * ar;
     }
     T out;
     out.x = (R)re;
     out.y = (R)im;
-    l[y] = out;
-    const T p = s[y];
-    e += (double)p.x * re + (double)p.y * im;
+    __stcs(l + y, out);
+    if (last) {
+      const T p = __ldcs(s + y);
+      e += (double)p.x * re + (double)p.y * im;
+    }
   }
+  if (!last) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
@@ -306,7 +323,7 @@ __global__ void __launch_bounds__(kAThreads)
   if (threadIdx.x == 0) {
     double v = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[w];
-    partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = v;
+    epart[((size_t)blockIdx.y * 2 + h) * gridDim.x + blockIdx.x] += v;
   }
 }
 
@@ -1485,30 +1502,40 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
     std::memcpy(h.data() + 20 * T_, coeffs, 8 * T_);
     KB_CUDA(cudaMemcpyAsync(hmeta.p, h.data(), h.size(), cudaMemcpyHostToDevice, st));
   }
-  // the terms with i^q folded into the coefficient, for ham_apply_smem
+  // the terms with i^q folded into the coefficient, grouped by the top
+  // qubit of their flip (ham_half; 0: same half, 1: other half)
   std::unique_ptr<DevBuf> d_ham;
-  if (T_ <= kHamSmemTerms) {
-    std::vector<HamTerm> ht(T_);
-    for (int t = 0; t < T_; ++t) {
-      const double c = coeffs[t];
-      ht[t].flip = flip[t];
-      ht[t].sign = sign[t];
-      switch (phq[t] & 3) {  // i^q
-        case 0: ht[t].cr = c, ht[t].ci = 0.0; break;
-        case 1: ht[t].cr = 0.0, ht[t].ci = c; break;
-        case 2: ht[t].cr = -c, ht[t].ci = 0.0; break;
-        default: ht[t].cr = 0.0, ht[t].ci = -c; break;
+  int ham_group0 = 0;
+  const bool ham_split = T_ <= kHamSmemTerms && n >= 1;
+  if (ham_split) {
+    std::vector<HamTerm> ht;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int t = 0; t < T_; ++t) {
+        if ((int)((flip[t] >> (n - 1)) & 1) != pass) continue;
+        HamTerm x;
+        const double c = coeffs[t];
+        x.flip = flip[t];
+        x.sign = sign[t];
+        switch (phq[t] & 3) {  // i^q
+          case 0: x.cr = c, x.ci = 0.0; break;
+          case 1: x.cr = 0.0, x.ci = c; break;
+          case 2: x.cr = -c, x.ci = 0.0; break;
+          default: x.cr = 0.0, x.ci = -c; break;
+        }
+        ht.push_back(x);
+        if (pass == 0) ++ham_group0;
       }
-    }
     d_ham = std::make_unique<DevBuf>(sizeof(HamTerm) * std::max(T_, 1));
     KB_CUDA(cudaMemcpyAsync(d_ham->p, ht.data(), sizeof(HamTerm) * T_, cudaMemcpyHostToDevice, st));
     static bool ham_attr[2] = {false, false};
     if (!ham_attr[sizeof(R) == 8]) {
-      KB_CUDA(cudaFuncSetAttribute(ham_apply_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      KB_CUDA(cudaFuncSetAttribute(ham_half<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(sizeof(HamTerm) * kHamSmemTerms)));
       ham_attr[sizeof(R) == 8] = true;
     }
   }
+  // ham_half grid: about one set's worth of resident CTAs per half
+  const int ham_ctas = (int)std::min<uint64_t>(std::max<uint64_t>(1, (dim / 2 + kAThreads - 1) / kAThreads), 148ull * 8);
   const uint64_t* d_flip = hmeta.as<uint64_t>();
   const uint64_t* d_sign = d_flip + T_;
   const int* d_q = reinterpret_cast<const int*>(d_sign + T_);
@@ -1616,9 +1643,12 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
       attr_set[sizeof(R) == 8] = true;
     }
   }
-  const size_t ham_doubles = chunk * blocks;
-  DevBuf part(sizeof(double) * (tiled ? grad_doubles + ham_doubles : chunk * blocks * (G + 1)));
-  double* d_ham_part = part.as<double>() + (tiled ? grad_doubles : (size_t)G * chunk * blocks);
+  const size_t ham_doubles = ham_split ? chunk * 2 * (size_t)ham_ctas : chunk * blocks;
+  // gradient partials (tiled: per block; per-gate: [gate][set][block]), then
+  // the expectation partials
+  const size_t grad_region = tiled ? grad_doubles : (size_t)G * chunk * blocks;
+  DevBuf part(sizeof(double) * (grad_region + ham_doubles));
+  double* d_ham_part = part.as<double>() + grad_region;
 
   std::vector<double> hmats(8 * chunk * std::max<size_t>(G, 1));
   std::vector<R> hmats_t(tiled ? hmats.size() : 0);  // the tiled sweeps read them in the state's precision
@@ -1665,14 +1695,28 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
     KB_CUDA(cudaGetLastError());
     // lambda = H psi and <H>
     {
-      dim3 grid((unsigned)blocks, (unsigned)nb);
-      if (T_ <= kHamSmemTerms)
-        ham_apply_smem<R><<<grid, kAThreads, sizeof(HamTerm) * T_, st>>>(psi.as<T>(), lam.as<T>(), dim,
-                                                                         d_ham->as<HamTerm>(), T_, d_ham_part);
-      else
+      if (ham_split) {
+        KB_CUDA(cudaMemsetAsync(d_ham_part, 0, sizeof(double) * ham_doubles, st));
+        const int g0 = ham_group0, g1 = T_ - ham_group0;
+        dim3 hgrid((unsigned)ham_ctas, (unsigned)nb);
+        for (int h = 0; h < 2; ++h) {
+          if (g0 > 0) {
+            ham_half<R><<<hgrid, kAThreads, sizeof(HamTerm) * g0, st>>>(
+                psi.as<T>(), lam.as<T>(), dim, h, 1, g1 == 0 ? 1 : 0, d_ham->as<HamTerm>(), g0, d_ham_part);
+            count_launch();
+          }
+          if (g1 > 0) {
+            ham_half<R><<<hgrid, kAThreads, sizeof(HamTerm) * g1, st>>>(
+                psi.as<T>(), lam.as<T>(), dim, h, g0 == 0 ? 1 : 0, 1, d_ham->as<HamTerm>() + g0, g1, d_ham_part);
+            count_launch();
+          }
+        }
+      } else {
+        dim3 grid((unsigned)blocks, (unsigned)nb);
         ham_apply<R><<<grid, kAThreads, 0, st>>>(psi.as<T>(), lam.as<T>(), dim, d_flip, d_sign, d_q, d_coef, T_,
                                                  d_ham_part);
-      count_launch();
+        count_launch();
+      }
     }
     // reverse sweep; at the last gate (block) of each segment, walking
     // backwards, psi is reset to the checkpoint of the segment's end
@@ -1704,15 +1748,16 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
       }
     }
     KB_CUDA(cudaGetLastError());
-    const size_t part_count = tiled ? grad_doubles + ham_doubles : (G + 1) * chunk * blocks;
+    const size_t part_count = grad_region + ham_doubles;
     hpart.resize(part_count);
     KB_CUDA(cudaMemcpyAsync(hpart.data(), part.p, sizeof(double) * part_count, cudaMemcpyDeviceToHost, st));
     KB_CUDA(cudaStreamSynchronize(st));
-    const double* hham = hpart.data() + (tiled ? grad_doubles : (size_t)G * chunk * blocks);
+    const double* hham = hpart.data() + grad_region;
     for (uint64_t b = 0; b < nb; ++b) {
       double v = 0;
-      const double* pv = hham + b * blocks;
-      for (int k = 0; k < blocks; ++k) v += pv[k];
+      const int per_set = ham_split ? 2 * ham_ctas : blocks;
+      const double* pv = hham + b * per_set;
+      for (int k = 0; k < per_set; ++k) v += pv[k];
       values[b0 + b] = v;
       double* gr = grads + (b0 + b) * nparams;
       for (uint64_t k = 0; k < nparams; ++k) gr[k] = 0.0;
