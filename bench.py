@@ -244,6 +244,19 @@ def run_sample33(args):
     plan.close()
 
 
+def _adjoint_blocks(n, ops, pidx):
+    """Number of tile blocks of the tiled adjoint sweep (complex64)."""
+    from ket_b200 import _lib
+    p = np.ascontiguousarray(pidx, dtype=np.int32)
+    length = ct.c_uint64()
+    _lib.check(_lib.lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), p.ctypes.data, _lib.C64, None, 0,
+                                                     ct.byref(length)))
+    out = np.zeros(length.value, dtype=np.int32)
+    _lib.check(_lib.lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), p.ctypes.data, _lib.C64,
+                                                     out.ctypes.data, length.value, ct.byref(length)))
+    return int(out[0])
+
+
 def run_adjoint24(args):
     """Adjoint gradients: 24-qubit, 8-layer Ry/Rz + CX-ring ansatz (384
     parameters), 64 random Pauli strings, a batch of 64 parameter sets;
@@ -265,9 +278,19 @@ def run_adjoint24(args):
         vals, grads = adjoint_expval(circ, pidx, theta, ham, "c64", 2)
         ts.append(time.perf_counter() - t0)
     t = statistics.median(ts)
+    # algorithmic HBM bytes per batch: per tile block and set, the forward
+    # reads and writes psi, the reverse psi and lambda; lambda = H psi reads
+    # psi and writes lambda once per set (its gathers beyond that are L2 hits)
+    blocks = _adjoint_blocks(n, circ.to_ops(), pidx)
+    state = 8 * 2 ** n
+    byts = batch * (blocks * (2 * state + 4 * state) + 2 * state)
+    peak, peak_kind = peaks()
     line = {"metric": "adjoint gradients/s (24q, 8 layers, 384 params, 64 Pauli terms, batch 64)",
             "value": batch * npar / t, "unit": "gradients/s", "higher_is_better": True,
-            "seconds_per_batch": t, "batch": batch, "params": npar}
+            "seconds_per_batch": t, "batch": batch, "params": npar,
+            "roofline": {"bound": "hbm", "achieved": byts / t / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": byts / t / 1e9 / peak, "peak_source": peak_kind, "traffic": None,
+                         "bytes_per_batch": byts, "tile_blocks": blocks}}
     if not args.no_checks:
         t0 = time.perf_counter()
         vpg, gpg = adjoint_expval(circ, pidx, theta, ham, "c64", 2, method="per_gate")
