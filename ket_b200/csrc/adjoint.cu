@@ -1309,16 +1309,20 @@ int pk_opcode_host(const TGate& g, bool rev) {
 std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGate>& gates, bool rev) {
   std::string o;
   auto line = [&](const std::string& x) { o += x + "\n"; };
-  line("extern \"C\" __global__ void __launch_bounds__(256, " + std::string(rev ? "1" : "2") + ")");
+  // Reverse: two CTAs per SM with one tile buffer each (load, compute,
+  // store) beat one CTA with two buffers: the other CTA's work covers the
+  // loads.  Forward: two CTAs, each prefetching its next tile.
+  line("extern \"C\" __global__ void __launch_bounds__(256, 2)");
   line("kb_tile_jit(float2* __restrict__ psi, float2* __restrict__ lam, uint64_t dim, kbt::TileGeom tg,");
   line("            const kbt::TGate* __restrict__ gates, int ngates, const float* __restrict__ mats,");
   line("            uint64_t mat_stride, int ngrad, double* __restrict__ partial) {");
   line("  using namespace kbt;");
   line(std::string("  constexpr bool REV = ") + (rev ? "true" : "false") + ";");
   line("  constexpr int TILE = 1 << TileCfg<float>::TB, BUF = (REV ? 2 : 1) * TILE;");
+  line("  constexpr bool SINGLE = REV;  // one tile buffer");
   line("  extern __shared__ __align__(16) unsigned char tsm[];");
   line("  float2* bufs = reinterpret_cast<float2*>(tsm);");
-  line("  f2* spk = reinterpret_cast<f2*>(tsm + 2 * BUF * sizeof(float2));");
+  line("  f2* spk = reinterpret_cast<f2*>(tsm + (SINGLE ? 1 : 2) * BUF * sizeof(float2));");
   line("  double* acc = reinterpret_cast<double*>(spk + 16 * ngates);");
   line("  __shared__ uint64_t off_lo[64], off_hi[64];");
   line("  const int tid = threadIdx.x;");
@@ -1328,15 +1332,17 @@ std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGat
   line("  c64_setup<REV>(tg, gates, ngates, mats, mat_stride, set, ngrad, off_lo, off_hi, spk, acc);");
   line("  __syncthreads();");
   line("  int cur = 0;");
-  line("  if (blockIdx.x < tg.n_tiles) c64_prefetch<REV>(tg, off_lo, off_hi, blockIdx.x, bufs, s, l);");
+  line("  if (!SINGLE && blockIdx.x < tg.n_tiles) c64_prefetch<REV>(tg, off_lo, off_hi, blockIdx.x, bufs, s, l);");
   line("  asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");");
   line("  for (uint64_t t = blockIdx.x; t < tg.n_tiles; t += gridDim.x) {");
-  line("    float2* sp = bufs + cur * BUF;");
+  line("    float2* sp = bufs + (SINGLE ? 0 : cur) * BUF;");
   line("    float2* sl = sp + TILE;");
-  line("    if (t + gridDim.x < tg.n_tiles)");
+  line("    if (SINGLE) c64_prefetch<REV>(tg, off_lo, off_hi, t, bufs, s, l);");
+  line("    else if (t + gridDim.x < tg.n_tiles)");
   line("      c64_prefetch<REV>(tg, off_lo, off_hi, t + gridDim.x, bufs + (cur ^ 1) * BUF, s, l);");
   line("    asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");");
-  line("    asm volatile(\"cp.async.wait_group 1;\\n\" ::: \"memory\");");
+  line("    if (SINGLE) asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");");
+  line("    else asm volatile(\"cp.async.wait_group 1;\\n\" ::: \"memory\");");
   line("    __syncthreads();");
   constexpr int TB = TileCfg<float>::TB;
   const int nph = (int)phases.size();
@@ -1387,7 +1393,8 @@ std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGat
 }
 
 size_t jit_smem(bool rev, int ngates, int ngrad) {
-  return (rev ? 4 : 2) * (size_t{1} << TileCfg<float>::TB) * sizeof(float2) + (size_t)ngates * 16 * sizeof(f2) +
+  // forward: two buffers of psi; reverse: one buffer of psi and lambda
+  return 2 * (size_t{1} << TileCfg<float>::TB) * sizeof(float2) + (size_t)ngates * 16 * sizeof(f2) +
          (rev ? (size_t)kTileWarps * ngrad * 8 : 0);
 }
 
