@@ -41,10 +41,11 @@ N_QUBITS, DEPTH, SEED = 30, 40, 1234
 METRIC = "time per 30q circuit"
 
 # DRAM bytes (read + write) of one fused_tc_kernel<5> launch on a 2^26
-# complex64 state, from ncu (dram__bytes_read.sum 537.14 MB +
-# dram__bytes_write.sum 476.98 MB, one launch of the 26-qubit depth-4 brick
-# wall).  A launch streams the state once, so the figure scales with 2^n.
-TC_TRAFFIC_BYTES_26Q = 537.143808e6 + 476.978944e6
+# complex64 state, from ncu (dram__bytes_read.sum 536.98 MB +
+# dram__bytes_write.sum 477.66 MB, one launch of the 26-qubit depth-4 brick
+# wall: the block on qubits 10..14).  A launch streams the state once, so the
+# figure scales with 2^n.
+TC_TRAFFIC_BYTES_26Q = 536.983552e6 + 477.661696e6
 
 
 def peaks():

@@ -138,6 +138,12 @@ int ketgpu_plan_execute_timed(const ketgpu_plan* p, ketgpu_state* s, float* pass
  * diagonal run touches), tensor-core flag and algorithmic HBM bytes. */
 int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* kind, int32_t* k,
                           int32_t* tensor, double* bytes);
+/* The qubits pass `index` acts on, ascending: a dense block's qubits (matrix
+ * bit b <-> qubits[b]), or a pair/phase pass's target and controls.  Writes
+ * min(count, capacity) entries; *count receives the full number (0 for norm
+ * passes and diagonal runs, which touch every qubit). */
+int ketgpu_plan_pass_qubits(const ketgpu_plan* p, uint64_t index, int32_t* qubits,
+                            int32_t capacity, int32_t* count);
 /* The state's CUDA stream (a cudaStream_t), for callers that order their
  * own work or events against the backend's. */
 void* ketgpu_state_stream(const ketgpu_state* s);

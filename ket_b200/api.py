@@ -448,6 +448,14 @@ class Plan:
         check(lib.ketgpu_plan_pass_info(self._h, index, ct.byref(kind), ct.byref(k), ct.byref(tc), ct.byref(b)))
         return {"kind": kind.value, "k": k.value, "tensor": bool(tc.value), "bytes": b.value}
 
+    def pass_qubits(self, index: int) -> List[int]:
+        """The qubits one pass acts on, ascending (dense block: matrix bit b is
+        qubits[b]); empty for norm passes and diagonal runs."""
+        buf = (ct.c_int32 * 8)()
+        cnt = ct.c_int32()
+        check(lib.ketgpu_plan_pass_qubits(self._h, index, buf, 8, ct.byref(cnt)))
+        return [buf[i] for i in range(min(cnt.value, 8))]
+
     def pass_bytes(self, index: int) -> float:
         return self.pass_info(index)["bytes"]
 

@@ -680,6 +680,28 @@ KB_API int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* 
   });
 }
 
+KB_API int ketgpu_plan_pass_qubits(const ketgpu_plan* p, uint64_t index, int32_t* qubits,
+                                   int32_t capacity, int32_t* count) {
+  return guard([&] {
+    need(p != nullptr && count != nullptr, "null argument");
+    need(capacity >= 0 && (capacity == 0 || qubits != nullptr), "bad qubit buffer");
+    const Plan& plan = *as_plan(p);
+    if (index >= plan.passes.size()) fail(KETGPU_ERR_OUT_OF_RANGE, "pass index out of range");
+    const Pass& ps = plan.passes[index];
+    const int* q = nullptr;
+    int nq = 0;
+    if (ps.kind == PassKind::Fused) {
+      q = ps.qubits;
+      nq = ps.k;
+    } else if (ps.kind == PassKind::Pair || ps.kind == PassKind::Phase) {
+      q = ps.fixed;
+      nq = ps.nfixed;
+    }
+    for (int i = 0; i < nq && i < capacity; ++i) qubits[i] = q[i];
+    *count = nq;
+  });
+}
+
 KB_API void* ketgpu_state_stream(const ketgpu_state* s) {
   return s ? reinterpret_cast<void*>(as_state(s)->stream) : nullptr;
 }

@@ -15,18 +15,21 @@
 // accumulated in FP32 in tensor memory (tcgen05.mma kind::tf32, M=128,
 // N=K=2^(k+1)).
 //
-// Pipeline (one CTA per SM, persistent over tiles, 256 threads):
-//   cp.async (16 B, coalesced) raw tiles into a 3-slot ring -> all threads
-//   split hi/lo into the 128B-swizzled K-major A images -> one thread issues
-//   the MMAs, tcgen05.commit signals an mbarrier -> while tile j's MMAs run,
-//   the CTA drains tile j-1's accumulator (double-buffered in TMEM) through
-//   shared memory back to global memory in address order.  Two tiles of
-//   loads stay in flight throughout.  Every mbarrier wait is bounded; on
-//   timeout the kernel raises an error flag, drains its copies, frees its
-//   tensor memory and returns.
+// Pipeline (one CTA per SM, persistent over tiles, warp-specialised):
+//   raw tiles into a ring of staging images -- one tiled tensor copy per
+//   tile when qubits 0..4 are group bits, per-thread cp.async otherwise ->
+//   converter warps split hi/lo into tensor memory -> one thread issues the
+//   MMAs, tcgen05.commit signals an mbarrier -> while tile j's MMAs run, the
+//   epilogue drains tile j-1's accumulator (double-buffered in TMEM) back to
+//   global memory, straight from registers or through shared memory.  Every
+//   mbarrier wait is bounded; on timeout the kernel raises an error flag,
+//   drains its copies, frees its tensor memory and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -73,6 +76,14 @@ struct TcGeom {
   int nh;             // tile qubits above the low run
   int hpos[16];
   int direct;         // the epilogue stores from registers (see launch_fused_tc)
+  // Tensor-copy producer (tma_dims > 0, see launch_tc): dimension i of the
+  // tensor map starts at qubit tma_start[i]; a tile's coordinate in it is
+  // (base >> tma_start[i]) & tma_mask[i].  ctile[c] = byte offset of
+  // combination c in the tile image (natural tile index order).
+  int tma_dims;
+  int tma_start[5];
+  uint64_t tma_mask[5];
+  uint32_t ctile[32];
   uint64_t cdep[32];  // offset of target combination c from its group's amplitude
   uint64_t n_tiles;
 };
@@ -102,6 +113,47 @@ __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
 }
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void* g) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr), "l"(g) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// One tiled tensor copy (2 to 5 dimensions, no multicast) of a whole box
+// into shared memory, completing its bytes on the mbarrier at `bar`.
+__device__ __forceinline__ void tma_load_box(uint32_t dst, const CUtensorMap* map, const int* c, int dims,
+                                             uint32_t bar) {
+  const uint64_t m = reinterpret_cast<uint64_t>(map);
+  switch (dims) {
+    case 2:
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+          "[%4];" ::"r"(dst),
+          "l"(m), "r"(c[0]), "r"(c[1]), "r"(bar)
+          : "memory");
+      break;
+    case 3:
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+          "%4}], [%5];" ::"r"(dst),
+          "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(bar)
+          : "memory");
+      break;
+    case 4:
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+          "%4, %5}], [%6];" ::"r"(dst),
+          "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(bar)
+          : "memory");
+      break;
+    default:
+      asm volatile(
+          "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+          "%4, %5, %6}], [%7];" ::"r"(dst),
+          "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(bar)
+          : "memory");
+      break;
+  }
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -169,7 +221,8 @@ __host__ __device__ constexpr uint32_t tf32_idesc() {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
-// Roles (13 warps): 0-3 producers (cp.async into staging images), 4-7
+// Roles (13 warps): 0-3 producers (cp.async into staging images; with a
+// tensor map, thread 0 alone issues one tiled copy per tile), 4-7
 // converters (hi/lo split into the A images), 8-11 epilogue (TMEM -> staging
 // -> HBM; warp w reads TMEM lanes 32*(w%4)..+31), 12 the MMA issuer.
 // mbarriers hand each tile from stage to stage, so loads of later tiles,
@@ -179,7 +232,8 @@ constexpr int kProducers = 128, kConverters = 128, kEpilogue = 128;
 
 template <int KQ>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    fused_tc_kernel(float2* __restrict__ s, TcGeom g, const uint32_t* __restrict__ bimg) {
+    fused_tc_kernel(float2* __restrict__ s, TcGeom g, const uint32_t* __restrict__ bimg,
+                    const __grid_constant__ CUtensorMap tmap) {
   using Cfg = TcCfg<KQ>;
   constexpr int N = Cfg::N, TILE = Cfg::TILE;
   constexpr int CPT = TILE / 2 / kProducers;  // 16-byte chunks per producer / epilogue thread
@@ -204,7 +258,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
   if (tid == 0) {
     for (int i = 0; i < S; ++i) {
-      mbar_init(smem_u32(&bar_full[i]), kProducers + 1);
+      mbar_init(smem_u32(&bar_full[i]), g.tma_dims ? 1 : kProducers + 1);
       mbar_init(smem_u32(&bar_free[i]), kEpilogue);
     }
     for (int i = 0; i < 2; ++i) {
@@ -302,7 +356,44 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     return b;
   };
 
-  if (warp < 4) {
+  if (warp < 4 && g.tma_dims) {
+    // ------------------------------------------ producer, tensor-copy form
+    // One thread fetches each whole tile with a single tiled tensor copy;
+    // the image holds the tile in its natural index order.
+    if (tid == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap)) : "memory");
+      uint64_t issued = 0;
+      for (uint64_t j = 0; j < count; ++j) {
+        const int slot = (int)(j % S);
+        if (j >= (uint64_t)S && !wait(&bar_free[slot], (uint32_t)(((j / S) - 1) & 1))) break;
+        const uint64_t base = tile_base(first + j * stride);
+        base_ring[j % (2 * S)] = base;
+        const uint32_t bar = smem_u32(&bar_full[slot]);
+        mbar_arrive_expect_tx(bar, (uint32_t)Cfg::RAW_BYTES);
+        int crd[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) crd[i] = (int)((base >> g.tma_start[i]) & g.tma_mask[i]);
+        tma_load_box(smem_u32(raw + slot * Cfg::RAW_BYTES), &tmap, crd, g.tma_dims, bar);
+        issued = j + 1;
+      }
+      // Drain: every issued tile's copy lands before the CTA may leave (on
+      // the normal path the converters have already seen them all).
+      for (uint64_t j = issued > (uint64_t)S ? issued - S : 0; j < issued; ++j) {
+        const uint32_t a = smem_u32(&bar_full[j % S]);
+        for (uint32_t it = 0; it < kWaitLimit; ++it) {
+          uint32_t done;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+              "selp.u32 %0, 1, 0, p;\n\t}"
+              : "=r"(done)
+              : "r"(a), "r"((uint32_t)((j / S) & 1))
+              : "memory");
+          if (done) break;
+        }
+      }
+    }
+  } else if (warp < 4) {
     // ------------------------------------------------------------ producers
     uint64_t goff[CPT];
     uint32_t soff[CPT];
@@ -343,6 +434,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int lane_row = 32 * q + lane;
     const int row = g.direct ? ((lane_row >> 1) | ((lane_row & 1) << (kGroupBits - 1))) : lane_row;
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+    // tensor-copy images: byte offset of this lane's group in the tile
+    uint32_t gtile = 0;
+    for (int jb = 0, gb = 0; jb < Cfg::TB; ++jb)
+      if (!g.is_target[jb]) {
+        if ((lane_row >> gb) & 1) gtile |= 8u << jb;
+        ++gb;
+      }
     for (uint64_t j = 0; j < count; ++j) {
       const int slot = (int)(j % S);
       if (!wait(&bar_full[slot], (uint32_t)((j / S) & 1))) break;
@@ -353,16 +451,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
       for (int part = 0; part < K / 16; ++part) {
         uint32_t hi[16], lo[16];
+        uint32_t xs[16];
+        if (g.tma_dims) {
+          // natural tile order, qubits 0..4 group bits: a warp's 32 lanes
+          // read 256 contiguous bytes per combination
 #pragma unroll
-        for (int c4 = 0; c4 < 4; ++c4) {
-          const uint4 x = *reinterpret_cast<const uint4*>(img + sw128_offset(row, part * 16 + 4 * c4, 128));
-          const uint32_t xs[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const uint32_t h = (xs[u] + 0x1000u) & 0xffffe000u;
-            hi[4 * c4 + u] = h;
-            lo[4 * c4 + u] = (__float_as_uint(__uint_as_float(xs[u]) - __uint_as_float(h)) + 0x1000u) & 0xffffe000u;
+          for (int i = 0; i < 8; ++i) {
+            const uint2 x = *reinterpret_cast<const uint2*>(img + g.ctile[part * 8 + i] + gtile);
+            xs[2 * i] = x.x;
+            xs[2 * i + 1] = x.y;
           }
+        } else {
+#pragma unroll
+          for (int c4 = 0; c4 < 4; ++c4) {
+            const uint4 x = *reinterpret_cast<const uint4*>(img + sw128_offset(row, part * 16 + 4 * c4, 128));
+            xs[4 * c4] = x.x;
+            xs[4 * c4 + 1] = x.y;
+            xs[4 * c4 + 2] = x.z;
+            xs[4 * c4 + 3] = x.w;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const uint32_t h = (xs[u] + 0x1000u) & 0xffffe000u;
+          hi[u] = h;
+          lo[u] = (__float_as_uint(__uint_as_float(xs[u]) - __uint_as_float(h)) + 0x1000u) & 0xffffe000u;
         }
         tmem_st16(areg + (uint32_t)(part * 16), hi);
         tmem_st16(areg + (uint32_t)(K + part * 16), lo);
@@ -476,6 +589,71 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// KETGPU_TC_TMA=0 keeps every block on the cp.async producers (for
+// comparing the two producer forms on one workload).
+bool tc_tma_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("KETGPU_TC_TMA");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// Tensor map over the state whose box is one tile: each dimension is a run
+// of consecutive tile qubits (at most 8, the box limit of 256 elements)
+// followed by the non-tile qubits up to the next run, so a tile's
+// coordinates are the non-tile bits of its base and the box lands in
+// shared memory in the tile's natural index order.  Returns the number of
+// dimensions, or 0 when the tile needs more than 5 or no encoder exists.
+int encode_tile_map(const State& st, TcGeom& g, int tb, CUtensorMap* map) {
+  if (!tc_tma_enabled()) return 0;
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return 0;
+  int start[16], tq[16], nd = 0;
+  for (int j = 0; j < tb; ++j) {
+    const int q = g.tile_pos[j];
+    if (j == 0 || q != g.tile_pos[j - 1] + 1 || tq[nd - 1] == 8) {
+      start[nd] = q;
+      tq[nd] = 0;
+      ++nd;
+    }
+    ++tq[nd - 1];
+  }
+  if (nd < 2 || nd > 5 || start[0] != 0) return 0;
+  cuuint64_t dims[5], strides[4];
+  cuuint32_t box[5], estr[5];
+  for (int i = 0; i < nd; ++i) {
+    const int end = i + 1 < nd ? start[i + 1] : st.n;
+    dims[i] = cuuint64_t{1} << (end - start[i]);
+    box[i] = 1u << tq[i];
+    estr[i] = 1;
+    if (i > 0) strides[i - 1] = (cuuint64_t{8}) << start[i];
+    g.tma_start[i] = start[i];
+    g.tma_mask[i] = dims[i] - 1;
+  }
+  for (int i = nd; i < 5; ++i) {
+    g.tma_start[i] = 0;
+    g.tma_mask[i] = 0;
+  }
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)nd, st.amps, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? nd : 0;
+}
+
 int sm_count_tc(int device) {
   int v = 0;
   KB_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
@@ -525,6 +703,20 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   g.nh = 0;
   for (int i = g.m_low; i < Cfg::TB; ++i) g.hpos[g.nh++] = g.tile_pos[i];
   g.n_tiles = st.dim() >> Cfg::TB;
+  CUtensorMap tmap;
+  std::memset(&tmap, 0, sizeof(tmap));
+  g.tma_dims = (p.qubits[0] >= 5 && g.direct) ? encode_tile_map(st, g, Cfg::TB, &tmap) : 0;
+  if (g.tma_dims) {
+    for (int c = 0; c < Cfg::DIM; ++c) {
+      uint32_t off = 0;
+      for (int b = 0, jb = 0; jb < Cfg::TB; ++jb)
+        if (g.is_target[jb]) {
+          if ((c >> b) & 1) off |= 8u << jb;
+          ++b;
+        }
+      g.ctile[c] = off;
+    }
+  }
   static int attr_done[64] = {0};
   if (st.device >= 0 && st.device < 64 && !(attr_done[st.device] & (1 << KQ))) {
     KB_CUDA(cudaFuncSetAttribute(fused_tc_kernel<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -536,7 +728,7 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   uint64_t grid = (uint64_t)sms[st.device];
   if (grid > g.n_tiles) grid = g.n_tiles;
   fused_tc_kernel<KQ><<<(unsigned)grid, kTcThreads, Cfg::SMEM, st.stream>>>(
-      static_cast<float2*>(st.amps), g, static_cast<const uint32_t*>(b_image));
+      static_cast<float2*>(st.amps), g, static_cast<const uint32_t*>(b_image), tmap);
   count_launch();
   KB_CUDA(cudaGetLastError());
 }

@@ -98,6 +98,31 @@ def test_plans_on_the_host():
     assert gr["bytes"] < un["bytes"] / 8
 
 
+def test_pass_qubits_describe_the_blocks():
+    """Each dense block of the 30-qubit brick wall reports its qubits in
+    ascending order; together the blocks cover every qubit."""
+    import ket_b200 as ket
+    from ket_b200.api import Plan
+    from ket_b200.workloads import random_brickwork
+    c = random_brickwork(30, 40)
+    p = Plan(30, c.to_ops(), ket.make_options("c64", "greedy", 5, True))
+    seen = set()
+    n_tc = 0
+    for i in range(p.stats()["n_passes"]):
+        info, qs = p.pass_info(i), p.pass_qubits(i)
+        if info["kind"] == 2:
+            assert len(qs) == info["k"] and qs == sorted(set(qs)) and 0 <= qs[0] and qs[-1] < 30
+            n_tc += info["tensor"]
+            seen |= set(qs)
+        elif info["kind"] in (3, 4):
+            assert qs == []
+        else:
+            assert 1 <= len(qs) <= 3
+    assert n_tc == 144 and seen == set(range(30))
+    with pytest.raises(Exception):
+        p.pass_qubits(10**6)
+
+
 def test_diagonal_runs_in_the_plan():
     """The 33-qubit QFT-pattern circuit: the 528 CP gates form one diagonal
     pass; the brick wall (no diagonal gates) is planned as before."""
