@@ -453,11 +453,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         uint32_t hi[16], lo[16];
         uint32_t xs[16];
         if (g.tma_dims) {
-          // natural tile order, qubits 0..4 group bits: a warp's 32 lanes
-          // read 256 contiguous bytes per combination
+          // natural tile order under the 128-byte swizzle (16-byte chunk
+          // c of 128-byte row r sits at chunk c ^ (r mod 8)), which spreads
+          // lanes whose groups lie 128 B apart or more over the banks
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            const uint2 x = *reinterpret_cast<const uint2*>(img + g.ctile[part * 8 + i] + gtile);
+            const uint32_t off = g.ctile[part * 8 + i] | gtile;
+            const uint2 x = *reinterpret_cast<const uint2*>(img + (off ^ ((off >> 3) & 0x70u)));
             xs[2 * i] = x.x;
             xs[2 * i + 1] = x.y;
           }
@@ -492,8 +494,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int row = 32 * q + lane;
     if (g.direct) {
       // TMEM lane = group `row`; the lanes of a warp vary the five lowest
-      // group bits, all within qubits 0..5, so a warp's 8-byte stores land
-      // within 512 contiguous bytes.
+      // group bits, which include qubits 0 and 1, so each run of lanes
+      // fills whole 32-byte sectors.
       uint64_t gdep = 0;
       for (int jb = 0, gb = 0; jb < Cfg::TB; ++jb)
         if (!g.is_target[jb]) {
@@ -602,37 +604,43 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// KETGPU_TC_TMA=0 keeps every block on the cp.async producers (for
-// comparing the two producer forms on one workload).
-bool tc_tma_enabled() {
-  static const bool on = [] {
+// Lowest target qubit from which a block uses the tensor-copy producer
+// (default 2: qubits 0 and 1 group bits).  KETGPU_TC_TMA=0 keeps every block
+// on the cp.async producers, KETGPU_TC_TMA_MIN=q raises the threshold (for
+// comparing the producer forms on one workload).
+int tc_tma_min() {
+  static const int v = [] {
     const char* e = std::getenv("KETGPU_TC_TMA");
-    return !(e && e[0] == '0');
+    if (e && e[0] == '0') return 1 << 20;
+    const char* m = std::getenv("KETGPU_TC_TMA_MIN");
+    const int q = m ? std::atoi(m) : 2;
+    return q < 2 ? 2 : q;
   }();
-  return on;
+  return v;
 }
 
 // Tensor map over the state whose box is one tile: each dimension is a run
-// of consecutive tile qubits (at most 8, the box limit of 256 elements)
-// followed by the non-tile qubits up to the next run, so a tile's
-// coordinates are the non-tile bits of its base and the box lands in
-// shared memory in the tile's natural index order.  Returns the number of
-// dimensions, or 0 when the tile needs more than 5 or no encoder exists.
+// of consecutive tile qubits followed by the non-tile qubits up to the next
+// run, so a tile's coordinates are the non-tile bits of its base and the box
+// lands in shared memory in the tile's natural index order, under the
+// 128-byte swizzle.  The first dimension is qubits 0..3 (128 bytes, the
+// swizzle's row); the others hold at most 8 tile qubits (the box limit of
+// 256 elements).  Returns the number of dimensions, or 0 when the tile needs
+// more than 5 or no encoder exists.
 int encode_tile_map(const State& st, TcGeom& g, int tb, CUtensorMap* map) {
-  if (!tc_tma_enabled()) return 0;
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc) return 0;
   int start[16], tq[16], nd = 0;
   for (int j = 0; j < tb; ++j) {
     const int q = g.tile_pos[j];
-    if (j == 0 || q != g.tile_pos[j - 1] + 1 || tq[nd - 1] == 8) {
+    if (j == 0 || q != g.tile_pos[j - 1] + 1 || tq[nd - 1] == (nd == 1 ? 4 : 8)) {
       start[nd] = q;
       tq[nd] = 0;
       ++nd;
     }
     ++tq[nd - 1];
   }
-  if (nd < 2 || nd > 5 || start[0] != 0) return 0;
+  if (nd < 2 || nd > 5 || start[0] != 0 || tq[0] != 4) return 0;
   cuuint64_t dims[5], strides[4];
   cuuint32_t box[5], estr[5];
   for (int i = 0; i < nd; ++i) {
@@ -649,7 +657,7 @@ int encode_tile_map(const State& st, TcGeom& g, int tb, CUtensorMap* map) {
     g.tma_mask[i] = 0;
   }
   const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)nd, st.amps, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? nd : 0;
 }
@@ -687,7 +695,8 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   // and the five lowest group bits lie within qubits 0..5: a warp's 32
   // stores then fill 32-byte sectors within 512 contiguous bytes.  Otherwise
   // (qubit 0 a target, or the lanes spread thin) the output is staged
-  // through shared memory and written in 16-byte words.
+  // through shared memory and written in 16-byte words.  Blocks that take
+  // the tensor-copy producer (qubits 0 and 1 group bits) store directly.
   {
     int seen = 0, fifth = 64;
     for (int b = 0; b < Cfg::TB && seen < 5; ++b)
@@ -705,8 +714,10 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   g.n_tiles = st.dim() >> Cfg::TB;
   CUtensorMap tmap;
   std::memset(&tmap, 0, sizeof(tmap));
-  g.tma_dims = (p.qubits[0] >= 5 && g.direct) ? encode_tile_map(st, g, Cfg::TB, &tmap) : 0;
+  // Tensor-copy blocks (qubits 0 and 1 group bits) always store directly.
+  g.tma_dims = p.qubits[0] >= tc_tma_min() ? encode_tile_map(st, g, Cfg::TB, &tmap) : 0;
   if (g.tma_dims) {
+    g.direct = 1;
     for (int c = 0; c < Cfg::DIM; ++c) {
       uint32_t off = 0;
       for (int b = 0, jb = 0; jb < Cfg::TB; ++jb)
