@@ -151,9 +151,17 @@ void* ketgpu_state_stream(const ketgpu_state* s);
 int ketgpu_apply(ketgpu_state* s, const ketgpu_op* ops, uint64_t n_ops,
                  const ketgpu_options* opt);
 /* ket::run with host buffers: |0...0>, the circuit, then the 2^n amplitudes
- * as complex128 into out_c128 (simulator.hpp:15, simulator.cpp:554-558). */
+ * as complex128 into out_c128 (simulator.hpp:15, simulator.cpp:554-558).
+ * The device state is kept after the call and reused by the next call of
+ * the same size, precision and device: freeing a 30-qubit state costs
+ * 150-700 ms.  A state allocation that would not fit frees it first, and
+ * ketgpu_release_cache frees it at once.  Concurrent calls each use their
+ * own state. */
 int ketgpu_run(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
                const ketgpu_options* opt, double* out_c128);
+/* Free the device state that ketgpu_run keeps between calls (no-op when
+ * there is none).  No counterpart in ket, whose run holds no device memory. */
+int ketgpu_release_cache(void);
 
 /* ---- reductions (FP64 accumulation) --------------------------------- */
 int ketgpu_norm(const ketgpu_state* s, double* out);

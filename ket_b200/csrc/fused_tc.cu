@@ -614,7 +614,7 @@ int tc_tma_min() {
     if (e && e[0] == '0') return 1 << 20;
     const char* m = std::getenv("KETGPU_TC_TMA_MIN");
     const int q = m ? std::atoi(m) : 2;
-    return q < 2 ? 2 : q;
+    return q < 0 ? 0 : q;
   }();
   return v;
 }

@@ -291,3 +291,25 @@ def test_edge_cases_like_ket():
     c2.t(1)
     c2.measure_all()
     assert len(ket.sample_shots(c2, 0, seed=1)) == 0
+
+
+def test_run_reuses_its_device_state(golden):
+    """ketgpu_run keeps its device state between calls: every call still
+    starts from |0...0>, whatever size, precision or release came before."""
+    import ctypes as ct
+    from ket_b200 import _lib
+    g = golden("random_mixed")
+
+    def run(n, precision):
+        out = np.zeros(1 << n, dtype=np.complex128)
+        opt = ket.make_options(precision, "greedy", 5, True)
+        ops = g[f"ops_{n}"]
+        _lib.check(_lib.lib.ketgpu_run(n, ops.ctypes.data, len(ops), ct.byref(opt), out.ctypes.data))
+        return out
+
+    tol = {"c128": 1e-12, "c64": 1e-5}
+    for n, precision in [(12, "c128"), (12, "c128"), (10, "c128"), (12, "c64"), (12, "c64"), (12, "c128")]:
+        assert np.abs(run(n, precision) - g[f"state_{n}"]).max() < tol[precision], (n, precision)
+    _lib.check(_lib.lib.ketgpu_release_cache())
+    _lib.check(_lib.lib.ketgpu_release_cache())
+    assert np.abs(run(12, "c64") - g["state_12"]).max() < 1e-5
