@@ -11,6 +11,7 @@
 #include <atomic>
 #include <barrier>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -240,9 +241,26 @@ bool have_avx512() {
 }
 
 // Pinned staging for complex64 downloads, kept for the life of the process:
-// three buffers of kDownChunk amplitudes (96 MB).  One download at a time
-// uses it.
-constexpr uint64_t kDownChunk = uint64_t{1} << 22;
+// a ring of down_ring() buffers of down_chunk() amplitudes (default 4 x 16 MB),
+// all but one of them in flight.  One download at a time uses it.  At 30
+// qubits 4 x 16 MB matched the raw copy (157-160 ms against 162 ms to pinned
+// memory); 3 x 32 MB took 181-188 ms and 4 x 8 MB 213-243 ms, the widening
+// no longer hidden behind the copy.  KETGPU_DOWN_CHUNK_MB and
+// KETGPU_DOWN_RING override the shape (read once).
+uint64_t env_u64(const char* name, uint64_t def, uint64_t lo, uint64_t hi) {
+  const char* e = std::getenv(name);
+  if (!e) return def;
+  const uint64_t v = std::strtoull(e, nullptr, 10);
+  return v < lo ? lo : (v > hi ? hi : v);
+}
+uint64_t down_chunk() {
+  static const uint64_t v = env_u64("KETGPU_DOWN_CHUNK_MB", 16, 1, 256) * (uint64_t{1} << 20) / 8;
+  return v;
+}
+int down_ring() {
+  static const int v = (int)env_u64("KETGPU_DOWN_RING", 4, 2, 16);
+  return v;
+}
 std::mutex g_stage_mu;
 void* g_stage = nullptr;
 
@@ -254,21 +272,23 @@ void download(const State& s, uint64_t first, uint64_t count, double* out) {
     return;
   }
   std::lock_guard<std::mutex> lock(g_stage_mu);
-  if (!g_stage) KB_CUDA(cudaMallocHost(&g_stage, 3 * kDownChunk * 8));
-  float2* buf[3];
-  for (int b = 0; b < 3; ++b) buf[b] = static_cast<float2*>(g_stage) + b * kDownChunk;
-  cudaEvent_t ev[3];
+  const uint64_t chunk = down_chunk();
+  const int ring = down_ring();
+  if (!g_stage) KB_CUDA(cudaMallocHost(&g_stage, ring * chunk * 8));
+  std::vector<float2*> buf(ring);
+  for (int b = 0; b < ring; ++b) buf[b] = static_cast<float2*>(g_stage) + b * chunk;
+  std::vector<cudaEvent_t> ev(ring);
   for (auto& e : ev) KB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  const uint64_t nchunks = (count + kDownChunk - 1) / kDownChunk;
+  const uint64_t nchunks = (count + chunk - 1) / chunk;
   cudaError_t err = cudaSuccess;  // no throw while the workers run
   auto issue = [&](uint64_t c) {
-    const uint64_t lo = c * kDownChunk, len = std::min(kDownChunk, count - lo);
-    cudaError_t e = cudaMemcpyAsync(buf[c % 3], static_cast<const float2*>(s.amps) + first + lo, len * 8,
+    const uint64_t lo = c * chunk, len = std::min(chunk, count - lo);
+    cudaError_t e = cudaMemcpyAsync(buf[c % ring], static_cast<const float2*>(s.amps) + first + lo, len * 8,
                                     cudaMemcpyDeviceToHost, s.stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[c % 3], s.stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[c % ring], s.stream);
     if (e != cudaSuccess && err == cudaSuccess) err = e;
   };
-  // Chunk c is widened by every worker while chunks c+1 and c+2 are in
+  // Chunk c is widened by every worker while chunks c+1 .. c+ring-1 are in
   // flight.  The workers start once per download and step through the
   // chunks between two barriers; the calling thread is worker 0 and also
   // issues the copies.
@@ -276,12 +296,12 @@ void download(const State& s, uint64_t first, uint64_t count, double* out) {
                                                   : std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
   const bool wide = have_avx512();
   auto slice = [&](unsigned t, uint64_t c) {
-    const uint64_t lo = c * kDownChunk, len = std::min(kDownChunk, count - lo);
+    const uint64_t lo = c * chunk, len = std::min(chunk, count - lo);
     // in floats, rounded to 16 floats (64 bytes of output) per worker
     const uint64_t nf = 2 * len, per = ((nf + nt - 1) / nt + 15) / 16 * 16;
     const uint64_t a = std::min(nf, t * per), b = std::min(nf, a + per);
     if (b > a)
-      (wide ? widen_avx512 : widen_scalar)(reinterpret_cast<const float*>(buf[c % 3]) + a, out + 2 * lo + a, b - a);
+      (wide ? widen_avx512 : widen_scalar)(reinterpret_cast<const float*>(buf[c % ring]) + a, out + 2 * lo + a, b - a);
   };
   std::barrier sync(nt);
   auto work = [&](unsigned t) {
@@ -293,13 +313,13 @@ void download(const State& s, uint64_t first, uint64_t count, double* out) {
   };
   std::vector<std::thread> th;
   for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
-  for (uint64_t c = 0; c < std::min<uint64_t>(2, nchunks); ++c) issue(c);
+  for (uint64_t c = 0; c < std::min<uint64_t>(ring - 1, nchunks); ++c) issue(c);
   for (uint64_t c = 0; c < nchunks; ++c) {
     if (err == cudaSuccess) {
-      const cudaError_t e = cudaEventSynchronize(ev[c % 3]);
+      const cudaError_t e = cudaEventSynchronize(ev[c % ring]);
       if (e != cudaSuccess) err = e;
     }
-    if (c + 2 < nchunks && err == cudaSuccess) issue(c + 2);
+    if (c + ring - 1 < nchunks && err == cudaSuccess) issue(c + ring - 1);
     sync.arrive_and_wait();
     slice(0, c);
     sync.arrive_and_wait();
