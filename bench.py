@@ -42,10 +42,10 @@ METRIC = "time per 30q circuit"
 
 # DRAM bytes (read + write) of one fused_tc_kernel<5> launch on a 2^26
 # complex64 state, from ncu (dram__bytes_read.sum 536.98 MB +
-# dram__bytes_write.sum 477.66 MB, one launch of the 26-qubit depth-4 brick
+# dram__bytes_write.sum 477.04 MB, one launch of the 26-qubit depth-4 brick
 # wall: the block on qubits 10..14).  A launch streams the state once, so the
 # figure scales with 2^n.
-TC_TRAFFIC_BYTES_26Q = 536.983552e6 + 477.661696e6
+TC_TRAFFIC_BYTES_26Q = 536.983808e6 + 477.042688e6
 
 
 def peaks():
