@@ -222,6 +222,13 @@ class Reference:
         L.ref_simulate_sample.argtypes = [i32, vp, sz, u32, i32, sz, vp, vp, ct.c_char_p, sz]
         L.ref_is_clifford.argtypes = [i32, vp, sz, vp]
         L.ref_chosen_method.argtypes = [i32, vp, sz, vp]
+        for name in ("ref_qasm_parse", "ref_qasm_roundtrip", "ref_to_qasm"):
+            if not hasattr(L, name):  # built before the OpenQASM entry points
+                break
+        else:
+            L.ref_qasm_parse.argtypes = [ct.c_char_p, vp, vp, vp, vp, sz, vp]
+            L.ref_qasm_roundtrip.argtypes = [ct.c_char_p, vp, sz, vp]
+            L.ref_to_qasm.argtypes = [i32, vp, sz, vp, sz, vp]
         self.L = L
 
     def _check(self, rc):
@@ -316,3 +323,36 @@ class Reference:
         out = ct.c_int(0)
         self._check(self.L.ref_chosen_method(n, ops.ctypes.data, len(ops), ct.byref(out)))
         return "stabilizer" if out.value == 2 else "statevector"
+
+    # -- OpenQASM (bindings/qasm/qasm.cpp) -----------------------------------
+    def qasm_parse(self, src):
+        """ket::from_qasm: register sizes, top-level node count and the gates
+        with composites expanded (barriers keep their width in nq)."""
+        nq, nc, top, n = ct.c_int(), ct.c_int(), ct.c_int(), ct.c_size_t()
+        ops = np.zeros(4096, dtype=OP_DTYPE)
+        b = src.encode()
+        self._check(self.L.ref_qasm_parse(b, ct.byref(nq), ct.byref(nc), ct.byref(top), ops.ctypes.data,
+                                          len(ops), ct.byref(n)))
+        if n.value > len(ops):
+            ops = np.zeros(n.value, dtype=OP_DTYPE)
+            self._check(self.L.ref_qasm_parse(b, ct.byref(nq), ct.byref(nc), ct.byref(top), ops.ctypes.data,
+                                              len(ops), ct.byref(n)))
+        return {"n_qubits": nq.value, "n_clbits": nc.value, "n_top": top.value, "ops": ops[:n.value].copy()}
+
+    def _text(self, call):
+        size = ct.c_size_t()
+        buf = ct.create_string_buffer(1 << 16)
+        self._check(call(buf, len(buf), ct.byref(size)))
+        if size.value >= len(buf):
+            buf = ct.create_string_buffer(size.value + 1)
+            self._check(call(buf, len(buf), ct.byref(size)))
+        return buf.raw[:size.value].decode()
+
+    def qasm_roundtrip(self, src):
+        """ket::to_qasm(ket::from_qasm(src))."""
+        b = src.encode()
+        return self._text(lambda buf, cap, n: self.L.ref_qasm_roundtrip(b, buf, cap, n))
+
+    def to_qasm(self, n, ops):
+        """ket::to_qasm of a circuit built from flat ops."""
+        return self._text(lambda buf, cap, k: self.L.ref_to_qasm(n, ops.ctypes.data, len(ops), buf, cap, k))

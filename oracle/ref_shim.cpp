@@ -10,7 +10,7 @@
 //     which shows ket's unchanged API running on the GPU backend.
 // Either way the code below only calls ket's public API
 // (include/ket/circuit.hpp, simulator.hpp, measurement.hpp, observable.hpp,
-// backends/backend.hpp, parallelism.hpp).
+// backends/backend.hpp, parallelism.hpp, qasm.hpp).
 #include <chrono>
 #include <cstddef>
 #include <cstdint>
@@ -26,6 +26,7 @@
 #include <ket/measurement.hpp>
 #include <ket/observable.hpp>
 #include <ket/parallelism.hpp>
+#include <ket/qasm.hpp>
 #include <ket/simulator.hpp>
 #include <ket/state.hpp>
 
@@ -263,5 +264,80 @@ SHIM_API int ref_chosen_method(int n, const ko_op* ops, std::size_t nops,
                                int* out) {
   return guard([&] {
     *out = ket::chosen_method(build(n, ops, nops)) == ket::Method::Stabilizer ? 2 : 1;
+  });
+}
+
+namespace {
+
+// A parsed circuit's gates with composites expanded through their wire map
+// (as simulator.cpp:504-511 expands them), one ko_op each.  A barrier keeps
+// its qubit count in nq and its first three qubits in q; a measure keeps its
+// classical bit in q[1].
+void flatten(const ket::Circuit& c, const std::vector<std::size_t>& wire, std::vector<ko_op>& out) {
+  for (const ket::DagNode& node : c.dag().nodes()) {
+    const ket::Gate& g = node.gate;
+    if (g.type == ket::GateType::Composite) {
+      if (!g.definition) continue;
+      std::vector<std::size_t> sub;
+      for (const auto& q : g.qubits) sub.push_back(wire[q.index]);
+      flatten(*g.definition, sub, out);
+      continue;
+    }
+    ko_op o{};
+    o.type = static_cast<int32_t>(g.type);
+    o.nq = static_cast<int32_t>(g.qubits.size());
+    for (std::size_t k = 0; k < g.qubits.size() && k < 3; ++k)
+      o.q[k] = static_cast<int32_t>(wire[g.qubits[k].index]);
+    if (g.type == ket::GateType::Measure) o.q[1] = static_cast<int32_t>(g.clbit);
+    for (std::size_t k = 0; k < g.params.size() && k < 3; ++k) o.p[k] = g.params[k];
+    out.push_back(o);
+  }
+}
+
+}  // namespace
+
+// ket::from_qasm (bindings/qasm/qasm.cpp:479-544), flattened: the register
+// sizes, the number of top-level nodes and up to cap ops (n_out = all).
+SHIM_API int ref_qasm_parse(const char* src, int* n_qubits, int* n_clbits, int* n_top, ko_op* out,
+                            std::size_t cap, std::size_t* n_out) {
+  return guard([&] {
+    const ket::Circuit c = ket::from_qasm(src);
+    std::vector<std::size_t> wire(c.n_qubits());
+    for (std::size_t i = 0; i < wire.size(); ++i) wire[i] = i;
+    std::vector<ko_op> ops;
+    flatten(c, wire, ops);
+    *n_qubits = static_cast<int>(c.n_qubits());
+    *n_clbits = static_cast<int>(c.n_clbits());
+    *n_top = static_cast<int>(c.dag().nodes().size());
+    for (std::size_t i = 0; i < ops.size() && i < cap; ++i) out[i] = ops[i];
+    *n_out = ops.size();
+  });
+}
+
+// ket::to_qasm(ket::from_qasm(src)) (qasm.cpp:764-780) into buf; len = the
+// full length, of which min(len, cap - 1) bytes and a terminator are written.
+SHIM_API int ref_qasm_roundtrip(const char* src, char* buf, std::size_t cap, std::size_t* len) {
+  return guard([&] {
+    const std::string text = ket::to_qasm(ket::from_qasm(src));
+    *len = text.size();
+    if (cap > 0) {
+      const std::size_t n = text.size() < cap - 1 ? text.size() : cap - 1;
+      std::memcpy(buf, text.data(), n);
+      buf[n] = '\0';
+    }
+  });
+}
+
+// ket::to_qasm of a circuit built from flat ops (no composites).
+SHIM_API int ref_to_qasm(int n, const ko_op* ops, std::size_t nops, char* buf, std::size_t cap,
+                         std::size_t* len) {
+  return guard([&] {
+    const std::string text = ket::to_qasm(build(n, ops, nops));
+    *len = text.size();
+    if (cap > 0) {
+      const std::size_t k = text.size() < cap - 1 ? text.size() : cap - 1;
+      std::memcpy(buf, text.data(), k);
+      buf[k] = '\0';
+    }
   });
 }

@@ -4,11 +4,12 @@ Run in a checkout where the reference sources are available:
     make -C oracle ref          # builds oracle/_ref/libket_ref.so from ket's sources
     python tests/golden/make_golden.py
 Every fixture is the output of ket's own code (ket::run, ket::expval,
-ket::measure, ket::sample) called through oracle/ref_shim.cpp; the circuits
-are seeded and stored next to the outputs.
+ket::measure, ket::sample, ket::from_qasm, ket::to_qasm) called through
+oracle/ref_shim.cpp; the circuits are seeded and stored next to the outputs.
 """
 from __future__ import annotations
 
+import json
 import math
 import os
 import sys
@@ -18,7 +19,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from oracle.oracle import ARITY, GATES, NPARAMS, Reference, make_ops  # noqa: E402
+from oracle.oracle import ARITY, CODE, GATES, NPARAMS, Reference, make_ops  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 
@@ -59,6 +60,48 @@ def brickwork_ops(n, depth, seed):
         for a in range(layer % 2, n - 1, 2):
             gs.append(("CX", [a, a + 1]))
     return make_ops(gs)
+
+
+def _hexops(ops):
+    return [[int(o["type"]), int(o["nq"])] + [int(v) for v in o["q"]] + [float(v).hex() for v in o["p"]]
+            for o in ops]
+
+
+def qasm_golden(R):
+    """ket::from_qasm / ket::to_qasm on the programs of qasm_programs.py:
+    the parsed circuit (flattened), its to_qasm text, ket::run's state for
+    the programs without measurements, the rejections, and to_qasm's angle
+    formatting."""
+    sys.path.insert(0, OUT)
+    from qasm_programs import ANGLES, ERRORS, PROGRAMS
+    progs = []
+    for name, src in PROGRAMS:
+        r = R.qasm_parse(src)
+        entry = {"name": name, "source": src, "n_qubits": r["n_qubits"], "n_clbits": r["n_clbits"],
+                 "n_top": r["n_top"], "ops": _hexops(r["ops"]), "to_qasm": R.qasm_roundtrip(src)}
+        ops = r["ops"]
+        finite = bool(np.isfinite(ops["p"]).all()) if len(ops) else True
+        if finite and not (ops["type"] == CODE["Measure"]).any() and r["n_qubits"] <= 8:
+            st = R.run(r["n_qubits"], ops)
+            entry["state"] = [[float(z.real).hex(), float(z.imag).hex()] for z in st]
+        progs.append(entry)
+    errs = []
+    for name, src in ERRORS:
+        try:
+            R.qasm_parse(src)
+        except Exception as e:  # noqa: BLE001 -- the rejection is the fixture
+            errs.append({"name": name, "source": src, "kind": type(e).__name__, "message": str(e)})
+        else:
+            raise AssertionError(f"ket accepted {name}")
+    angles = []
+    for a in ANGLES:
+        ops = make_ops([("Rz", [0], [a]), ("U", [0], [a, -a, 2 * a]), ("CP", [0, 1], [a])])
+        angles.append({"angle": float(a).hex(), "to_qasm": R.to_qasm(2, ops)})
+    mixed = make_ops([("H", [0]), ("CU", [1, 2], [0.5, math.pi / 3, -math.pi]), ("Measure", [2, 3]),
+                      ("Barrier", []), ("Probe", []), ("CSwap", [0, 1, 2]), ("Measure", [0, 0])])
+    with open(os.path.join(OUT, "qasm.json"), "w") as f:
+        json.dump({"programs": progs, "errors": errs, "angles": angles,
+                   "mixed": {"n": 3, "ops": _hexops(mixed), "to_qasm": R.to_qasm(3, mixed)}}, f, indent=1)
 
 
 def main():
@@ -113,8 +156,13 @@ def main():
     sv = R.sample(4, circ, 123, 200, method=1)
     au = R.sample(4, circ, 123, 200, method=0)
     np.savez_compressed(os.path.join(OUT, "sample.npz"), ops=circ, statevector=sv, auto=au)
+    # 7. OpenQASM: ket::from_qasm and ket::to_qasm
+    qasm_golden(R)
     print("golden fixtures written to", OUT)
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["qasm"]:  # only the OpenQASM fixture
+        qasm_golden(Reference())
+    else:
+        main()

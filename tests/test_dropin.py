@@ -112,3 +112,28 @@ def test_clifford_circuits_stay_on_kets_stabilizer():
     b, name_d = D.sample(3, ops, 11, 200, method=0, evolve_once=True)
     assert name_r == name_d == "stabilizer"
     assert np.array_equal(a, b)
+
+
+def _qasm_programs():
+    import json
+    with open(os.path.join(os.path.dirname(__file__), "golden", "qasm.json")) as f:
+        return json.load(f)["programs"]
+
+
+def test_qasm_reads_and_writes_through_kets_own_parser():
+    """ket::from_qasm / to_qasm are ket's, unchanged, in the drop-in build."""
+    _, D = _libs()
+    for prog in _qasm_programs():
+        assert D.qasm_roundtrip(prog["source"]) == prog["to_qasm"], prog["name"]
+
+
+@pytest.mark.gpu
+def test_qasm_programs_run_on_the_gpu_through_ket():
+    """ket's parser feeding ket::run on the B200 backend."""
+    _, D = _libs()
+    for prog in _qasm_programs():
+        if "state" not in prog:
+            continue
+        r = D.qasm_parse(prog["source"])
+        want = np.array([complex(float.fromhex(a), float.fromhex(b)) for a, b in prog["state"]])
+        assert np.abs(D.run(r["n_qubits"], r["ops"]) - want).max() < 1e-12, prog["name"]
