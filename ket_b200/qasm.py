@@ -107,11 +107,15 @@ def _statements(src: str) -> List[str]:
 
 
 def _stoul(text: str) -> int:
-    """std::stoul on an already trimmed string: the leading decimal digits."""
-    m = re.match(r"[" + re.escape(_SPACE) + r"]*\+?([0-9]+)", text)
+    """std::stoul on an already trimmed string: the leading decimal digits,
+    a minus sign wrapping modulo 2^64 as strtoul does."""
+    m = re.match(r"[" + re.escape(_SPACE) + r"]*([+-]?)([0-9]+)", text)
     if not m:
         raise ValueError("stoul")
-    return int(m.group(1))
+    v = int(m.group(2))
+    if v >= 1 << 64:
+        raise IndexError("stoul")  # out of range (std::out_of_range)
+    return (-v) % (1 << 64) if m.group(1) == "-" else v
 
 
 # ---------------------------------------------------------------- angles
@@ -146,9 +150,11 @@ def _number_prefix(s: str, pos: int) -> Optional[Tuple[float, int]]:
 def _fdiv(a: float, b: float) -> float:
     try:
         return a / b
-    except ZeroDivisionError:  # IEEE 754 division, as in C++
-        if a == 0.0 or math.isnan(a):
-            return math.nan
+    except ZeroDivisionError:  # IEEE 754 division, as the C++ parser does it
+        if math.isnan(a):
+            return a
+        if a == 0.0:
+            return math.inf - math.inf  # the hardware's default NaN, as 0.0/0.0
         return math.copysign(math.inf, a) * math.copysign(1.0, b)
 
 
@@ -421,6 +427,8 @@ def from_qasm(source: str) -> Circuit:
         elif head == "gate":
             name, d = _gate_def(st)
             defs.setdefault(name, d)
+    if qreg.total >= 1 << 63:  # a wrapped negative size: ket's vector allocation refuses it
+        raise ValueError("cannot create std::vector larger than max_size()")
     c = Circuit(qreg.total)
     for st in stmts:
         head = _head(st)
@@ -465,6 +473,8 @@ def _angle_text(a: float) -> str:
             if den != 1:
                 t += f"/{den}"
             return "-" + t if num < 0 else t
+    if math.isnan(a):  # C's printf shows the sign of a NaN
+        return "-nan" if math.copysign(1.0, a) < 0 else "nan"
     return "%.15g" % a
 
 

@@ -70,7 +70,16 @@ late q[1], q[0];
 creg c[0];
 """),
     ("divide_by_zero_angle", HEADER + """qreg q[1];
-rz(1/0) q[0]; rx(-1/0) q[0];
+rz(1/0) q[0]; rx(-1/0) q[0]; ry(0/0) q[0]; rz(1/-0) q[0];
+"""),
+    ("number_forms", HEADER + """qreg q[1];
+rx(0x1.8p1) q[0]; rx(1.e5) q[0]; rz(0X.4P+3) q[0]; ry(007) q[0];
+"""),
+    ("builtins_shadow_user_gates", HEADER + """gate h a { x a; }
+gate k(b) y { g(b+1) y; g(-b) y; }
+gate g(a) x { rz(a*2) x; }
+qreg q[2];
+h q[0]; k(0.5) q[1]; k(0.5) q[0]; k(0.25) q[0];
 """),
     ("brick_wall_5q", HEADER + """qreg q[5];
 U(0.11,0.22,0.33) q[0]; U(1.1,2.2,3.3) q[1]; U(0.5,0.6,0.7) q[2]; U(2.0,1.0,0.5) q[3]; U(0.9,0.8,0.7) q[4];
@@ -89,6 +98,11 @@ ERRORS = [
     ("measure_without_arrow", "qreg q[1]; creg c[1]; measure q[0] c[0];"),
     ("unknown_register", "qreg q[1]; x r[0];"),
     ("index_out_of_range", "qreg q[2]; h q[2];"),
+    ("negative_index", "qreg q[2]; h q[-1];"),
+    ("angle_overflow", "qreg q[1]; rx(1e999) q[0];"),
+    ("angle_underflow", "qreg q[1]; rx(1e-310) q[0];"),
+    ("angle_dangling_exponent", "qreg q[1]; rx(1e+) q[0];"),
+    ("angle_bare_hex_prefix", "qreg q[1]; rz(0x) q[0];"),
     ("unindexed_operand", "qreg q[2]; h q;"),
     ("malformed_declaration", "qreg q;"),
     ("wrong_qubit_count", "qreg q[3]; cx q[0];"),
