@@ -11,6 +11,7 @@ fusion mode and the tensor-core path.
 from __future__ import annotations
 
 import ctypes as ct
+import math
 import os
 import threading
 from typing import Iterable, List, Optional, Sequence, Tuple, Union
@@ -191,6 +192,24 @@ class DeviceState:
         return torch.as_tensor(_CAI(), device="cuda").view(dt)
 
 
+def _num_text(x: float) -> str:
+    if math.isnan(x):  # C's printf shows the sign of a NaN
+        return "-nan" if math.copysign(1.0, x) < 0 else "nan"
+    return "%g" % x
+
+
+def _amp_text(z: complex) -> str:
+    """An amplitude as ket writes it (src/state.cpp:20-32)."""
+    re_, im = z.real, z.imag
+    if im == 0.0:
+        return _num_text(re_)
+    if re_ == 0.0:
+        return _num_text(im) + "i"
+    if im < 0.0:
+        return f"{_num_text(re_)} - {_num_text(-im)}i"
+    return f"{_num_text(re_)} + {_num_text(im)}i"
+
+
 class State:
     """ket.State: 2^n complex128 amplitudes on the host (state.hpp:15-34),
     keeping the device copy it was produced from for further queries."""
@@ -209,6 +228,18 @@ class State:
 
     def __repr__(self):
         return f"<ket_b200.State size={len(self._amps)}>"
+
+    def print(self) -> str:
+        """ket.State.print (src/state.cpp:42-52): one line per amplitude,
+        ``|b_{n-1}...b_0⟩: amplitude``, numbers as C++ streams write a double
+        by default (6 significant digits)."""
+        n = 0
+        while (1 << n) < len(self._amps):
+            n += 1
+        return "".join(f"|{format(i, f'0{n}b') if n else ''}⟩: {_amp_text(z)}\n"
+                       for i, z in enumerate(self._amps.tolist()))
+
+    __str__ = print
 
     def to_numpy(self) -> np.ndarray:
         return self._amps

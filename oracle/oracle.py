@@ -222,13 +222,14 @@ class Reference:
         L.ref_simulate_sample.argtypes = [i32, vp, sz, u32, i32, sz, vp, vp, ct.c_char_p, sz]
         L.ref_is_clifford.argtypes = [i32, vp, sz, vp]
         L.ref_chosen_method.argtypes = [i32, vp, sz, vp]
-        for name in ("ref_qasm_parse", "ref_qasm_roundtrip", "ref_to_qasm"):
+        for name in ("ref_qasm_parse", "ref_qasm_roundtrip", "ref_to_qasm", "ref_state_print"):
             if not hasattr(L, name):  # built before the OpenQASM entry points
                 break
         else:
             L.ref_qasm_parse.argtypes = [ct.c_char_p, vp, vp, vp, vp, sz, vp]
             L.ref_qasm_roundtrip.argtypes = [ct.c_char_p, vp, sz, vp]
             L.ref_to_qasm.argtypes = [i32, vp, sz, vp, sz, vp]
+            L.ref_state_print.argtypes = [i32, vp, vp, sz, vp]
         self.L = L
 
     def _check(self, rc):
@@ -356,3 +357,8 @@ class Reference:
     def to_qasm(self, n, ops):
         """ket::to_qasm of a circuit built from flat ops."""
         return self._text(lambda buf, cap, k: self.L.ref_to_qasm(n, ops.ctypes.data, len(ops), buf, cap, k))
+
+    def state_print(self, n, state):
+        """ket::State::print of 2^n complex amplitudes."""
+        a = np.ascontiguousarray(state, dtype=np.complex128)
+        return self._text(lambda buf, cap, k: self.L.ref_state_print(n, a.ctypes.data, buf, cap, k))

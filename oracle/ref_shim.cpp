@@ -341,3 +341,16 @@ SHIM_API int ref_to_qasm(int n, const ko_op* ops, std::size_t nops, char* buf, s
     }
   });
 }
+
+// ket::State::print (src/state.cpp:42-52) of 2^n amplitudes.
+SHIM_API int ref_state_print(int n, const double* amps, char* buf, std::size_t cap, std::size_t* len) {
+  return guard([&] {
+    const std::string text = to_state(n, amps).print();
+    *len = text.size();
+    if (cap > 0) {
+      const std::size_t k = text.size() < cap - 1 ? text.size() : cap - 1;
+      std::memcpy(buf, text.data(), k);
+      buf[k] = '\0';
+    }
+  });
+}

@@ -4,8 +4,9 @@ Run in a checkout where the reference sources are available:
     make -C oracle ref          # builds oracle/_ref/libket_ref.so from ket's sources
     python tests/golden/make_golden.py
 Every fixture is the output of ket's own code (ket::run, ket::expval,
-ket::measure, ket::sample, ket::from_qasm, ket::to_qasm) called through
-oracle/ref_shim.cpp; the circuits are seeded and stored next to the outputs.
+ket::measure, ket::sample, ket::from_qasm, ket::to_qasm, ket::State::print)
+called through oracle/ref_shim.cpp; the circuits are seeded and stored next
+to the outputs.
 """
 from __future__ import annotations
 
@@ -104,6 +105,20 @@ def qasm_golden(R):
                    "mixed": {"n": 3, "ops": _hexops(mixed), "to_qasm": R.to_qasm(3, mixed)}}, f, indent=1)
 
 
+def state_print_golden(R):
+    """ket::State::print on generic and edge-valued states."""
+    special = np.array([0.0, -0.0, 1.0, -1.0, 1j, -1j, 0.5 - 0.25j, 1e-30 + 1e30j,
+                        -0.0 + 0.3j, 0.1 - 0.0j, 123456789.0, 1.5e-7 - 2.25e-8j, 0.25 + 1e-300j,
+                        -7.125 + 7.125j, 2.0 ** -20, 3.0 - 1e20j])
+    rng = np.random.default_rng(11)
+    cases = [(0, np.array([1.0 + 0.0j])), (1, np.array([0.6, -0.8j])), (4, special),
+             (6, rng.standard_normal(64) + 1j * rng.standard_normal(64))]
+    out = [{"n": n, "state": [[float(z.real).hex(), float(z.imag).hex()] for z in st],
+            "text": R.state_print(n, st)} for n, st in cases]
+    with open(os.path.join(OUT, "state_print.json"), "w") as f:
+        json.dump(out, f, indent=1, ensure_ascii=False)
+
+
 def main():
     R = Reference()
     # 1. gate battery: every gate, three operand orders, 4 qubits
@@ -158,11 +173,14 @@ def main():
     np.savez_compressed(os.path.join(OUT, "sample.npz"), ops=circ, statevector=sv, auto=au)
     # 7. OpenQASM: ket::from_qasm and ket::to_qasm
     qasm_golden(R)
+    # 8. State::print
+    state_print_golden(R)
     print("golden fixtures written to", OUT)
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] == ["qasm"]:  # only the OpenQASM fixture
+    if sys.argv[1:] == ["qasm"]:  # only the OpenQASM and State::print fixtures
         qasm_golden(Reference())
+        state_print_golden(Reference())
     else:
         main()

@@ -108,3 +108,16 @@ def test_composites_are_named_blocks():
     text = ket.to_qasm(c2)
     assert "gate r q0 {" in text and "gate r_2 q0 {" in text
     assert text.endswith("r q[0];\nr_2 q[1];\nr q[1];\n")
+
+
+def test_state_print_like_ket():
+    """State.print / str(State) write what ket::State::print writes
+    (tests/golden/state_print.json)."""
+    import numpy as np
+    from ket_b200.api import State
+    with open(os.path.join(os.path.dirname(__file__), "golden", "state_print.json")) as f:
+        cases = json.load(f)
+    for case in cases:
+        amps = np.array([complex(float.fromhex(a), float.fromhex(b)) for a, b in case["state"]])
+        assert State(amps).print() == case["text"], case["n"]
+        assert str(State(amps)) == case["text"]
