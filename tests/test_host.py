@@ -123,6 +123,14 @@ def test_pass_qubits_describe_the_blocks():
         p.pass_qubits(10**6)
 
 
+def test_release_cache_without_a_kept_state():
+    """ketgpu_release_cache is a no-op (and touches no device) when no
+    ketgpu_run call has kept a state."""
+    from ket_b200 import _lib
+    assert _lib.lib.ketgpu_release_cache() == 0
+    assert _lib.lib.ketgpu_release_cache() == 0
+
+
 def test_diagonal_runs_in_the_plan():
     """The 33-qubit QFT-pattern circuit: the 528 CP gates form one diagonal
     pass; the brick wall (no diagonal gates) is planned as before."""
