@@ -144,6 +144,14 @@ int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* kind, i
  * passes and diagonal runs, which touch every qubit). */
 int ketgpu_plan_pass_qubits(const ketgpu_plan* p, uint64_t index, int32_t* qubits,
                             int32_t capacity, int32_t* count);
+/* How tensor-core pass `index` runs: tma_dims = dimensions of the tensor map
+ * that fetches each tile with one tiled copy (0: per-thread cp.async), and
+ * direct = 1 when the epilogue stores straight from registers (0: staged
+ * through shared memory).  Assumes the driver provides cuTensorMapEncodeTiled.
+ * KETGPU_ERR_INVALID for a pass that is not a tensor-core block.  Host only;
+ * no counterpart in ket. */
+int ketgpu_plan_pass_tc_form(const ketgpu_plan* p, uint64_t index, int32_t* tma_dims,
+                             int32_t* direct);
 /* The state's CUDA stream (a cudaStream_t), for callers that order their
  * own work or events against the backend's. */
 void* ketgpu_state_stream(const ketgpu_state* s);

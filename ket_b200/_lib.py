@@ -79,6 +79,7 @@ def _load():
         "ketgpu_plan_pass_info": ([vp, u64, ct.POINTER(i32), ct.POINTER(i32), ct.POINTER(i32), pd], ct.c_int),
         "ketgpu_plan_pass_qubits": ([vp, u64, ct.POINTER(i32), i32, ct.POINTER(i32)], ct.c_int),
         "ketgpu_release_cache": ([], ct.c_int),
+        "ketgpu_plan_pass_tc_form": ([vp, u64, ct.POINTER(i32), ct.POINTER(i32)], ct.c_int),
         "ketgpu_state_stream": ([vp], vp),
         "ketgpu_apply": ([vp, vp, u64, ct.POINTER(Options)], ct.c_int),
         "ketgpu_run": ([i32, vp, u64, ct.POINTER(Options), vp], ct.c_int),

@@ -487,6 +487,14 @@ class Plan:
         check(lib.ketgpu_plan_pass_qubits(self._h, index, buf, 8, ct.byref(cnt)))
         return [buf[i] for i in range(min(cnt.value, 8))]
 
+    def pass_tc_form(self, index: int) -> dict:
+        """How a tensor-core pass runs: ``tma_dims`` (dimensions of the
+        tensor map fetching each tile; 0 = per-thread cp.async) and
+        ``direct`` (epilogue stores straight from registers)."""
+        t, d = ct.c_int32(), ct.c_int32()
+        check(lib.ketgpu_plan_pass_tc_form(self._h, index, ct.byref(t), ct.byref(d)))
+        return {"tma_dims": t.value, "direct": bool(d.value)}
+
     def pass_bytes(self, index: int) -> float:
         return self.pass_info(index)["bytes"]
 

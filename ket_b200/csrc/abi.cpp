@@ -764,6 +764,20 @@ KB_API int ketgpu_plan_pass_qubits(const ketgpu_plan* p, uint64_t index, int32_t
   });
 }
 
+KB_API int ketgpu_plan_pass_tc_form(const ketgpu_plan* p, uint64_t index, int32_t* tma_dims, int32_t* direct) {
+  return guard([&] {
+    need(p != nullptr && tma_dims != nullptr && direct != nullptr, "null argument");
+    const Plan& plan = *as_plan(p);
+    if (index >= plan.passes.size()) fail(KETGPU_ERR_OUT_OF_RANGE, "pass index out of range");
+    const Pass& ps = plan.passes[index];
+    if (ps.kind != PassKind::Fused || !ps.tensor) fail(KETGPU_ERR_INVALID, "pass is not a tensor-core block");
+    int t = 0, d = 0;
+    tc_form(plan.n, ps, &t, &d);
+    *tma_dims = t;
+    *direct = d;
+  });
+}
+
 KB_API void* ketgpu_state_stream(const ketgpu_state* s) {
   return s ? reinterpret_cast<void*>(as_state(s)->stream) : nullptr;
 }

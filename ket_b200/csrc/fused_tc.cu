@@ -627,10 +627,10 @@ int tc_tma_min() {
 // swizzle's row); the others hold at most 8 tile qubits (the box limit of
 // 256 elements).  Returns the number of dimensions, or 0 when the tile needs
 // more than 5 or no encoder exists.
-int encode_tile_map(const State& st, TcGeom& g, int tb, CUtensorMap* map) {
-  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc) return 0;
-  int start[16], tq[16], nd = 0;
+// The tensor map's dimensions for a tile (host only): start qubit and tile
+// qubits of each, returned count, or 0 when the tile does not fit the rules.
+int tile_runs(const TcGeom& g, int tb, int* start, int* tq) {
+  int nd = 0;
   for (int j = 0; j < tb; ++j) {
     const int q = g.tile_pos[j];
     if (j == 0 || q != g.tile_pos[j - 1] + 1 || tq[nd - 1] == (nd == 1 ? 4 : 8)) {
@@ -640,7 +640,15 @@ int encode_tile_map(const State& st, TcGeom& g, int tb, CUtensorMap* map) {
     }
     ++tq[nd - 1];
   }
-  if (nd < 2 || nd > 5 || start[0] != 0 || tq[0] != 4) return 0;
+  return (nd < 2 || nd > 5 || start[0] != 0 || tq[0] != 4) ? 0 : nd;
+}
+
+int encode_tile_map(const State& st, TcGeom& g, int tb, CUtensorMap* map) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return 0;
+  int start[16], tq[16];
+  const int nd = tile_runs(g, tb, start, tq);
+  if (!nd) return 0;
   cuuint64_t dims[5], strides[4];
   cuuint32_t box[5], estr[5];
   for (int i = 0; i < nd; ++i) {
@@ -668,22 +676,25 @@ int sm_count_tc(int device) {
   return v;
 }
 
+// Tile layout of a block on an n-qubit state (host only): the tile qubits,
+// the tile index decomposition, each combination's offset and the
+// cp.async-form direct-store rule.
 template <int KQ>
-void launch_tc(const State& st, const Pass& p, const void* b_image) {
+void tile_geometry(int n, const Pass& p, TcGeom& g) {
   using Cfg = TcCfg<KQ>;
-  TcGeom g{};
+  g = TcGeom{};
   uint64_t tmask = 0;
   for (int b = 0; b < p.k; ++b) tmask |= uint64_t{1} << p.qubits[b];
   uint64_t tiles_mask = tmask;
   int extra = Cfg::TB - p.k;
-  for (int q = 0; q < st.n && extra > 0; ++q)
+  for (int q = 0; q < n && extra > 0; ++q)
     if (!((tmask >> q) & 1)) {
       tiles_mask |= uint64_t{1} << q;
       --extra;
     }
   if (extra > 0) fail(KETGPU_ERR_LOGIC, "tensor-core block needs n >= k + 7");
   int j = 0;
-  for (int q = 0; q < st.n; ++q)
+  for (int q = 0; q < n; ++q)
     if ((tiles_mask >> q) & 1) {
       g.tile_pos[j] = q;
       g.is_target[j] = (int)((tmask >> q) & 1);
@@ -711,7 +722,14 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   }
   g.nh = 0;
   for (int i = g.m_low; i < Cfg::TB; ++i) g.hpos[g.nh++] = g.tile_pos[i];
-  g.n_tiles = st.dim() >> Cfg::TB;
+  g.n_tiles = (uint64_t{1} << n) >> Cfg::TB;
+}
+
+template <int KQ>
+void launch_tc(const State& st, const Pass& p, const void* b_image) {
+  using Cfg = TcCfg<KQ>;
+  TcGeom g;
+  tile_geometry<KQ>(st.n, p, g);
   CUtensorMap tmap;
   std::memset(&tmap, 0, sizeof(tmap));
   // Tensor-copy blocks (qubits 0 and 1 group bits) always store directly.
@@ -793,6 +811,17 @@ void launch_fused_tc(const State& s, const Pass& p, const void* b_image) {
   if (p.k == 5) launch_tc<5>(s, p, b_image);
   else if (p.k == 4) launch_tc<4>(s, p, b_image);
   else fail(KETGPU_ERR_LOGIC, "tensor-core block supports k = 4 or 5");
+}
+
+void tc_form(int n, const Pass& p, int* tma_dims, int* direct) {
+  if (p.k != 4 && p.k != 5) fail(KETGPU_ERR_LOGIC, "tensor-core block supports k = 4 or 5");
+  TcGeom g;
+  if (p.k == 5) tile_geometry<5>(n, p, g);
+  else tile_geometry<4>(n, p, g);
+  int start[16], tq[16];
+  const int nd = p.qubits[0] >= tc_tma_min() ? tile_runs(g, p.k + kGroupBits, start, tq) : 0;
+  *tma_dims = nd;
+  *direct = nd ? 1 : g.direct;
 }
 
 int tc_error_flag(bool reset) {

@@ -153,6 +153,11 @@ void learned_predict(const std::vector<float>& rows, std::vector<float>& us);
 void launch_pass(const State& s, const Plan& plan, const Pass& p);
 void upload_plan_matrices(Plan& plan, int device);
 void launch_fused_tc(const State& s, const Pass& p, const void* b_image);
+// Host only: the producer and epilogue forms a tensor-core launch of pass p
+// on an n-qubit state takes (tma_dims = tensor-map dimensions, 0 for the
+// cp.async producers; direct = register-to-HBM stores), given the tensor-map
+// encoder of the driver.
+void tc_form(int n, const Pass& p, int* tma_dims, int* direct);
 // Diagonal pass: device data = table (2^L complex, state precision) then FP64
 // coefficients, laid out by diag_device_data (diag.cu).
 void launch_diag(const State& s, const Pass& p, const void* data);

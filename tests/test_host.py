@@ -123,6 +123,47 @@ def test_pass_qubits_describe_the_blocks():
         p.pass_qubits(10**6)
 
 
+def test_tensor_core_producer_forms():
+    """Which tensor-core blocks fetch tiles with one tensor copy (and how many
+    tensor-map dimensions), and which store straight from registers: the
+    first tensor-copy dimension is qubits 0-3, later ones hold runs of at
+    most 8 tile qubits, at most 5 in all; blocks targeting qubit 0 or 1 keep
+    the cp.async producers."""
+    import collections
+    import ket_b200 as ket
+    from ket_b200.api import Plan
+    from ket_b200.workloads import random_brickwork
+    opt = ket.make_options("c64", "greedy", 5, True)
+    p = Plan(30, random_brickwork(30, 40).to_ops(), opt)
+    forms = collections.Counter()
+    for i in range(p.stats()["n_passes"]):
+        info = p.pass_info(i)
+        if info["kind"] == 2 and info["tensor"]:
+            f = p.pass_tc_form(i)
+            forms[(f["tma_dims"], f["direct"])] += 1
+            if f["tma_dims"]:
+                assert p.pass_qubits(i)[0] >= 2 and f["direct"]
+        else:
+            with pytest.raises(ValueError):
+                p.pass_tc_form(i)
+    assert forms == {(2, True): 20, (3, True): 66, (4, True): 40, (0, False): 18}
+
+    expect = {(10, 11, 12, 13, 14): (3, True), (5, 6, 23, 24, 25): (3, True), (8, 9, 10, 13, 14): (4, True),
+              (2, 3, 4, 5, 6): (2, True), (3, 4, 5, 14, 15): (3, True), (8, 10, 12, 14, 16): (0, True),
+              (3, 9, 14, 20, 27): (0, True), (1, 3, 5, 7, 9): (0, False), (0, 1, 2, 3, 4): (0, False)}
+    for qs, want in expect.items():
+        c = ket.Circuit(28)
+        for q in qs:
+            c.u(q, 0.3, 0.2, 0.1)
+        for a, b in zip(qs[:-1], qs[1:]):
+            c.cx(a, b)
+        p = Plan(28, c.to_ops(), opt)
+        tc = [i for i in range(p.stats()["n_passes"]) if p.pass_info(i)["tensor"]]
+        assert len(tc) == 1 and tuple(p.pass_qubits(tc[0])) == qs
+        f = p.pass_tc_form(tc[0])
+        assert (f["tma_dims"], f["direct"]) == want, qs
+
+
 def test_release_cache_without_a_kept_state():
     """ketgpu_release_cache is a no-op (and touches no device) when no
     ketgpu_run call has kept a state."""
