@@ -222,7 +222,8 @@ class Reference:
         L.ref_simulate_sample.argtypes = [i32, vp, sz, u32, i32, sz, vp, vp, ct.c_char_p, sz]
         L.ref_is_clifford.argtypes = [i32, vp, sz, vp]
         L.ref_chosen_method.argtypes = [i32, vp, sz, vp]
-        for name in ("ref_qasm_parse", "ref_qasm_roundtrip", "ref_to_qasm", "ref_state_print"):
+        for name in ("ref_qasm_parse", "ref_qasm_roundtrip", "ref_to_qasm", "ref_state_print",
+                     "ref_stepper_walk", "ref_stepper_seek"):
             if not hasattr(L, name):  # built before the OpenQASM entry points
                 break
         else:
@@ -230,6 +231,8 @@ class Reference:
             L.ref_qasm_roundtrip.argtypes = [ct.c_char_p, vp, sz, vp]
             L.ref_to_qasm.argtypes = [i32, vp, sz, vp, sz, vp]
             L.ref_state_print.argtypes = [i32, vp, vp, sz, vp]
+            L.ref_stepper_walk.argtypes = [i32, vp, sz, vp, sz, vp]
+            L.ref_stepper_seek.argtypes = [i32, vp, sz, vp, sz, vp, vp]
         self.L = L
 
     def _check(self, rc):
@@ -362,3 +365,21 @@ class Reference:
         """ket::State::print of 2^n complex amplitudes."""
         a = np.ascontiguousarray(state, dtype=np.complex128)
         return self._text(lambda buf, cap, k: self.L.ref_state_print(n, a.ctypes.data, buf, cap, k))
+
+    # -- Stepper (include/ket/stepper.hpp) ------------------------------------
+    def stepper_walk(self, n, ops):
+        """States at every position of ket::Stepper stepped to the end."""
+        cap = len(ops) + 1
+        out = np.zeros((cap, 1 << n), dtype=np.complex128)
+        steps = ct.c_size_t()
+        self._check(self.L.ref_stepper_walk(n, ops.ctypes.data, len(ops), out.ctypes.data, cap, ct.byref(steps)))
+        return out[:steps.value + 1]
+
+    def stepper_seek(self, n, ops, seq):
+        """ket::Stepper::seek(k) for each k of seq: (states, positions)."""
+        seq = np.ascontiguousarray(seq, dtype=np.uint64)
+        out = np.zeros((len(seq), 1 << n), dtype=np.complex128)
+        pos = np.zeros(len(seq), dtype=np.uint64)
+        self._check(self.L.ref_stepper_seek(n, ops.ctypes.data, len(ops), seq.ctypes.data, len(seq),
+                                            out.ctypes.data, pos.ctypes.data))
+        return out, pos

@@ -10,7 +10,7 @@
 //     which shows ket's unchanged API running on the GPU backend.
 // Either way the code below only calls ket's public API
 // (include/ket/circuit.hpp, simulator.hpp, measurement.hpp, observable.hpp,
-// backends/backend.hpp, parallelism.hpp, qasm.hpp).
+// backends/backend.hpp, parallelism.hpp, qasm.hpp, stepper.hpp).
 #include <chrono>
 #include <cstddef>
 #include <cstdint>
@@ -29,6 +29,7 @@
 #include <ket/qasm.hpp>
 #include <ket/simulator.hpp>
 #include <ket/state.hpp>
+#include <ket/stepper.hpp>
 
 #include "ketsv_oracle.h"
 
@@ -351,6 +352,41 @@ SHIM_API int ref_state_print(int n, const double* amps, char* buf, std::size_t c
       const std::size_t k = text.size() < cap - 1 ? text.size() : cap - 1;
       std::memcpy(buf, text.data(), k);
       buf[k] = '\0';
+    }
+  });
+}
+
+// ket::Stepper (include/ket/stepper.hpp:18-41) stepped to the end: the state
+// at every position 0..size() into out (up to cap states of 2^n amplitudes),
+// n_steps = size().  A step() past the end must return false.
+SHIM_API int ref_stepper_walk(int n, const ko_op* ops, std::size_t nops, double* out, std::size_t cap,
+                              std::size_t* n_steps) {
+  return guard([&] {
+    ket::Stepper s{build(n, ops, nops)};
+    *n_steps = s.size();
+    const std::size_t dim = std::size_t{1} << n;
+    std::size_t k = 0;
+    const auto record = [&] {
+      if (k < cap) from_state(s.state(), out + 2 * dim * k);
+      ++k;
+    };
+    record();
+    while (s.step()) record();
+    if (!s.at_end() || s.step()) throw std::logic_error("stepper: stepped past the end");
+  });
+}
+
+// ket::Stepper::seek(k) for each k of seq in turn: the state after each
+// (n_seq states of 2^n amplitudes) and pos() after each.
+SHIM_API int ref_stepper_seek(int n, const ko_op* ops, std::size_t nops, const std::size_t* seq,
+                              std::size_t n_seq, double* out, std::size_t* pos) {
+  return guard([&] {
+    ket::Stepper s{build(n, ops, nops)};
+    const std::size_t dim = std::size_t{1} << n;
+    for (std::size_t i = 0; i < n_seq; ++i) {
+      s.seek(seq[i]);
+      pos[i] = s.pos();
+      from_state(s.state(), out + 2 * dim * i);
     }
   });
 }

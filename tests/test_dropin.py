@@ -137,3 +137,30 @@ def test_qasm_programs_run_on_the_gpu_through_ket():
         r = D.qasm_parse(prog["source"])
         want = np.array([complex(float.fromhex(a), float.fromhex(b)) for a, b in prog["state"]])
         assert np.abs(D.run(r["n_qubits"], r["ops"]) - want).max() < 1e-12, prog["name"]
+
+
+@pytest.mark.gpu
+def test_stepper_steps_and_seeks_like_kets():
+    """ket::Stepper on the B200 backend against ket's own (tests/test_stepper.cpp:51-96
+    in ket): the state at every position when stepping to the end, then seeks
+    forward, backward, to the same place and past the end."""
+    R, D = _libs()
+    rng = np.random.default_rng(17)
+    gs = []
+    for i in range(40):
+        g = GATES[int(rng.integers(24))]
+        qs = rng.choice(5, ARITY[g], replace=False).tolist()
+        gs.append((g, qs, rng.uniform(0, 2 * math.pi, NPARAMS.get(g, 0)).tolist()))
+        if i % 9 == 4:
+            gs.append(("Barrier", []))
+        if i % 13 == 6:
+            gs.append(("Measure", [int(rng.integers(5)), i % 3]))
+    ops = make_ops(gs)
+    want, got = R.stepper_walk(5, ops), D.stepper_walk(5, ops)
+    assert want.shape == got.shape == (len(ops) + 1, 32)
+    assert np.abs(want - got).max() < 1e-12
+    size = len(ops)
+    seq = [size, 3, 0, size - 1, 5, 5, size + 10, 1, size // 2]
+    (sw, pw), (sg, pg) = R.stepper_seek(5, ops, seq), D.stepper_seek(5, ops, seq)
+    assert pw.tolist() == pg.tolist() == [min(k, size) for k in seq]
+    assert np.abs(sw - sg).max() < 1e-12

@@ -313,3 +313,25 @@ def test_run_reuses_its_device_state(golden):
     _lib.check(_lib.lib.ketgpu_release_cache())
     _lib.check(_lib.lib.ketgpu_release_cache())
     assert np.abs(run(12, "c64") - g["state_12"]).max() < 1e-5
+
+
+def test_repeated_runs_are_bit_identical(golden):
+    """The same circuit gives the same bits every time and whatever the thread
+    setting, as ket demands of its parallel runs (EXPECT_DOUBLE_EQ,
+    tests/test_parallelism.cpp:70-85): no reduction on the path depends on
+    scheduling."""
+    import ctypes as ct
+    from ket_b200 import _lib
+    ops = golden("random_mixed")["ops_12"]
+    try:
+        for precision in ("c128", "c64"):
+            opt = ket.make_options(precision, "greedy", 5, True)
+            runs = []
+            for threads in (1, 8, 0, 1):
+                ket.set_num_threads(threads)
+                out = np.zeros(1 << 12, dtype=np.complex128)
+                _lib.check(_lib.lib.ketgpu_run(12, ops.ctypes.data, len(ops), ct.byref(opt), out.ctypes.data))
+                runs.append(out)
+            assert all(np.array_equal(r, runs[0]) for r in runs[1:]), precision
+    finally:
+        ket.set_num_threads(1)
