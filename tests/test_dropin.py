@@ -164,3 +164,22 @@ def test_stepper_steps_and_seeks_like_kets():
     (sw, pw), (sg, pg) = R.stepper_seek(5, ops, seq), D.stepper_seek(5, ops, seq)
     assert pw.tolist() == pg.tolist() == [min(k, size) for k in seq]
     assert np.abs(sw - sg).max() < 1e-12
+
+
+@pytest.mark.gpu
+def test_stabilizer_equals_gpu_statevector_on_cliffords():
+    """ket's tableau and the B200 state vector agree on random Clifford
+    circuits for every Pauli string (ket's own check,
+    tests/test_stabilizer.cpp:91-106, seed 1234, 1e-9), both reached through
+    ket's expval(Circuit, PauliSum, Method)."""
+    import itertools
+    _, D = _libs()
+    clifford = ["H", "S", "Sdg", "X", "Y", "Z", "CX", "CY", "CZ", "Swap"]
+    n = 3
+    paulis = ["".join(p) for p in itertools.product("IXYZ", repeat=n)]
+    for seed in (1234, 1235, 1236, 1237):
+        ops = _random_ops(n, 40, seed, gates=clifford)
+        for p in paulis:
+            stab = D.expval_circuit(n, ops, [(1.0, p)], method=2)
+            sv = D.expval_circuit(n, ops, [(1.0, p)], method=1)
+            assert abs(stab - sv) < 1e-9, (seed, p)
