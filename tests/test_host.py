@@ -164,6 +164,27 @@ def test_tensor_core_producer_forms():
         assert (f["tma_dims"], f["direct"]) == want, qs
 
 
+def test_thread_count_api_like_ket():
+    """set_num_threads / num_threads behave as ket's (src/parallelism.cpp:164-169,
+    tests/test_parallelism.cpp:102-109): the default is 1, 0 means every
+    hardware thread, and the value reads back."""
+    import subprocess
+    import sys
+    import ket_b200 as ket
+    fresh = subprocess.run([sys.executable, "-c", "import ket_b200 as k; print(k.num_threads())"],
+                           capture_output=True, text=True, check=True)
+    assert fresh.stdout.strip() == "1"
+    try:
+        ket.set_num_threads(4)
+        assert ket.num_threads() == 4
+        ket.set_num_threads(0)
+        assert ket.num_threads() >= 1
+        ket.set_num_threads(1)
+        assert ket.num_threads() == 1
+    finally:
+        ket.set_num_threads(1)
+
+
 def test_release_cache_without_a_kept_state():
     """ketgpu_release_cache is a no-op (and touches no device) when no
     ketgpu_run call has kept a state."""
