@@ -359,7 +359,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp < 4 && g.tma_dims) {
     // ------------------------------------------ producer, tensor-copy form
     // One thread fetches each whole tile with a single tiled tensor copy;
-    // the image holds the tile in its natural index order.
+    // the image holds the tile in its natural index order under the
+    // 128-byte swizzle.
     if (tid == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap)) : "memory");
       uint64_t issued = 0;
@@ -625,10 +626,10 @@ int tc_tma_min() {
 // lands in shared memory in the tile's natural index order, under the
 // 128-byte swizzle.  The first dimension is qubits 0..3 (128 bytes, the
 // swizzle's row); the others hold at most 8 tile qubits (the box limit of
-// 256 elements).  Returns the number of dimensions, or 0 when the tile needs
-// more than 5 or no encoder exists.
-// The tensor map's dimensions for a tile (host only): start qubit and tile
-// qubits of each, returned count, or 0 when the tile does not fit the rules.
+// 256 elements); at most 5 dimensions.
+//
+// tile_runs (host only) returns the number of dimensions with each one's
+// start qubit and tile-qubit count, or 0 when the tile breaks those limits.
 int tile_runs(const TcGeom& g, int tb, int* start, int* tq) {
   int nd = 0;
   for (int j = 0; j < tb; ++j) {
@@ -643,6 +644,9 @@ int tile_runs(const TcGeom& g, int tb, int* start, int* tq) {
   return (nd < 2 || nd > 5 || start[0] != 0 || tq[0] != 4) ? 0 : nd;
 }
 
+// Encodes the map for one launch and fills g's coordinate fields; returns
+// the number of dimensions, or 0 (cp.async producers) when the tile breaks
+// the limits or the driver has no encoder.
 int encode_tile_map(const State& st, TcGeom& g, int tb, CUtensorMap* map) {
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc) return 0;
