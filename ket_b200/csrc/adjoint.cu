@@ -1485,6 +1485,10 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
   size_t free_b = 0, total_b = 0;
   KB_CUDA(cudaMemGetInfo(&free_b, &total_b));
   const size_t per_set = dim * sizeof(T) * (2 + (size_t)n_ckpt);
+  if ((uint64_t)((free_b * 0.6) / per_set) < batch) {  // first take back ketgpu_run's kept state
+    release_run_state();
+    KB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  }
   uint64_t chunk = std::max<uint64_t>(1, (uint64_t)((free_b * 0.6) / per_set));
   chunk = std::min<uint64_t>(chunk, batch);
   chunk = std::min<uint64_t>(chunk, 65535);

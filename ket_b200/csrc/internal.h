@@ -173,6 +173,8 @@ bool tc_supported(int k);
 void set_ground(const State& s);
 // Squared norm into a device scalar (partials: kNormBlocks doubles).
 void norm_to_device(const State& s, double* partials, double* out);
+// Free the device state that ketgpu_run keeps between calls (if any).
+void release_run_state();
 // s *= sqrt(target[0] / current[0]), factor read on the device.
 void rescale_state(const State& s, const double* target, const double* current);
 double reduce_norm(const State& s);
