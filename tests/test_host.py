@@ -147,6 +147,16 @@ def test_tensor_core_producer_forms():
             with pytest.raises(ValueError):
                 p.pass_tc_form(i)
     assert forms == {(2, True): 20, (3, True): 66, (4, True): 40, (0, False): 18}
+    # 4-qubit blocks (11-qubit tiles): the same rule
+    p4 = Plan(30, random_brickwork(30, 40).to_ops(), ket.make_options("c64", "greedy", 4, True))
+    for i in range(p4.stats()["n_passes"]):
+        info = p4.pass_info(i)
+        if info["kind"] == 2 and info["tensor"]:
+            assert info["k"] == 4
+            f = p4.pass_tc_form(i)
+            assert 0 <= f["tma_dims"] <= 5
+            assert (f["tma_dims"] > 0) == (p4.pass_qubits(i)[0] >= 2)
+            assert f["direct"] or f["tma_dims"] == 0
 
     expect = {(10, 11, 12, 13, 14): (3, True), (5, 6, 23, 24, 25): (3, True), (8, 9, 10, 13, 14): (4, True),
               (2, 3, 4, 5, 6): (2, True), (3, 4, 5, 14, 15): (3, True), (8, 10, 12, 14, 16): (0, True),
