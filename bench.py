@@ -16,9 +16,11 @@ Lines printed by rank 0 (one JSON line):
                complex128 buffer)
   roofline     the dense-block kernel: algorithmic bytes per launch / its
                mean CUDA-event duration, against MEASURED_PEAKS.json HBM
-  cpu_baseline ket itself (oracle/_ref/libket_ref.so, all host threads) on
-               a bounded sample of the same circuit, extrapolated
-  --impl reference   times ket's CPU path the same way and prints its line.
+  cpu_baseline ket itself (oracle/_ref/libket_ref.so, all host threads): one
+               full ket::run of the same circuit, timed; its complex128
+               state gives checks.max_abs_vs_ket / fidelity_vs_ket
+  --impl reference   full ket::run calls, one per step, as many as fit
+               --reference-budget seconds; prints its own line.
 """
 from __future__ import annotations
 
@@ -92,36 +94,28 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def cpu_baseline_reference(circ_ops, seconds_budget=20.0):
-    """ket::run (all host threads) on a bounded sample of the circuit.
-
-    The sample: ket::run of the empty 30-qubit circuit (state allocation),
-    then of prefixes holding only U gates and only CX gates; per-gate times
-    are extrapolated to the 1200 U + 580 CX of the full circuit.
-    """
-    from oracle.oracle import CODE, Reference
+def ket_full_run(ops, keep_state=False):
+    """One full ket::run of the circuit (oracle/_ref/libket_ref.so: ket built
+    from its own sources, set_num_threads(0) = every host thread), timed
+    around the call alone.  Returns (seconds, threads, state or None)."""
+    from oracle.oracle import Reference
     R = Reference()
     R.set_num_threads(0)
-    cores = R.num_threads()
-    u_ops = circ_ops[circ_ops["type"] == CODE["U"]]
-    cx_ops = circ_ops[circ_ops["type"] == CODE["CX"]]
-    t0 = R.run_timed(N_QUBITS, circ_ops[:0])
-    t_u1 = R.run_timed(N_QUBITS, u_ops[:1])
-    per_u = max(t_u1 - t0, 1e-6)
-    k_u = int(max(1, min(8, (seconds_budget * 0.5) // per_u)))
-    tu = R.run_timed(N_QUBITS, u_ops[:k_u])
-    per_u = max((tu - t0) / k_u, 1e-6)
-    k_cx = int(max(1, min(8, (seconds_budget * 0.3) // per_u)))
-    tcx = R.run_timed(N_QUBITS, cx_ops[:k_cx])
-    per_cx = max((tcx - t0) / k_cx, 1e-6)
-    n_u, n_cx = len(u_ops), len(cx_ops)
-    est = t0 + per_u * n_u + per_cx * n_cx
-    return {
-        "value": est * 1e3, "unit": "ms/circuit", "cores": cores, "kind": "reference",
-        "sample": (f"ket::run (oracle/_ref/libket_ref.so, set_num_threads(0)) at 30 qubits complex128: "
-                   f"empty circuit {t0:.2f} s, {k_u} U gates {tu:.2f} s, {k_cx} CX gates {tcx:.2f} s; "
-                   f"extrapolated {t0:.2f} + {n_u} x {per_u:.3f} + {n_cx} x {per_cx:.3f} s"),
-    }
+    threads = int(R.num_threads())
+    if keep_state:
+        secs, st = R.run_timed_state(N_QUBITS, ops)
+        return secs, threads, st
+    return R.run_timed(N_QUBITS, ops), threads, None
+
+
+def host_cpu():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def init_dist(n_gpus):
@@ -144,30 +138,44 @@ def barrier(world):
 
 
 def run_reference_arm(args):
-    rank, world, _ = init_dist(args.gpus)
-    if rank != 0:
-        barrier(world)
+    """ket's own CPU path on this workload: full ket::run calls of the 30-qubit
+    depth-40 brick wall (complex128, every host thread), one per step, as many
+    steps as fit in --reference-budget seconds (at least one).  Loads only
+    ket built from its sources (oracle/_ref) -- not the B200 package.  Under
+    torchrun only rank 0 runs; the other ranks exit without work."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return
-    from ket_b200.workloads import random_brickwork
-    ops = random_brickwork(N_QUBITS, DEPTH, SEED).to_ops()
-    vals = []
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
-    for _ in range(max(1, args.steps)):
-        vals.append(cpu_baseline_reference(ops, seconds_budget=10.0))
-    v = statistics.median([x["value"] for x in vals])
+    from oracle.oracle import Reference, brickwork_ops
+    R = Reference()
+    R.set_num_threads(0)
+    threads = int(R.num_threads())
+    ops = brickwork_ops(N_QUBITS, DEPTH, SEED, R.uniforms)
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max(1, args.steps):
+        times.append(R.run_timed(N_QUBITS, ops))
+        if time.perf_counter() - t_start + times[-1] > args.reference_budget:
+            break
+    v = statistics.median(times) * 1e3
+    sample = (f"{len(times)} full ket::run call(s) of the 30-qubit depth-40 brick wall (1200 U + 580 CX, "
+              f"complex128, 16 GiB state) through ket's public API (oracle/_ref/libket_ref.so built from "
+              f"ket's sources), set_num_threads(0) = {threads} threads on {host_cpu()}; each call timed "
+              f"alone: {', '.join(f'{t:.1f} s' for t in times)}")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "ms/circuit", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": "random U+CX brick wall, 30 qubits, depth 40, seed 1234",
-                   "global_batch": 1, "seq_len": None, "parallelism": "replicas"},
-        "cpu_baseline": {"value": v, "unit": "ms/circuit", "cores": vals[0]["cores"], "kind": "reference",
-                         "sample": vals[0]["sample"]},
+        "steps": len(times), "warmup": 0, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": v, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "random U+CX brick wall, 30 qubits, depth 40, seed 1234", "global_batch": 1,
+                   "seq_len": None, "parallelism": "host threads",
+                   "note": "a step is one full ket::run (about 7-8 minutes on 16 threads), so the run stops "
+                           "after the steps that fit the time budget and reports the steps it ran; no "
+                           "warm-up step (each call allocates its own state)"},
+        "cpu_baseline": {"value": v, "unit": "ms/circuit", "cores": threads, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": v, "unit": "ms/circuit", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-    barrier(world)
 
 
 def run_sample33(args):
@@ -353,7 +361,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--reference-budget", type=float, default=600.0,
+                    help="seconds of full ket::run calls in --impl reference (at least one call)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-checks", action="store_true")
     ap.add_argument("--fusion", default="greedy")
@@ -483,26 +493,53 @@ def main():
     if args.e2e_steps > 0:
         out = np.empty(1 << nq, dtype=np.complex128)
         ops_pinned = ops.copy()
-        ts = []
+        ts, profs = [], []
+        prof = np.zeros(6)
         for i in range(args.e2e_steps + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             _lib.check(lib.ketgpu_run(nq, ops_pinned.ctypes.data, len(ops_pinned), ct.byref(opt),
                                       out.ctypes.data))
             t1 = time.perf_counter()
+            _lib.check(lib.ketgpu_run_last_profile(prof.ctypes.data))
             if i > 0:
                 ts.append((t1 - t0) * 1e3)
+                profs.append(prof.copy())
         e2e_ms = barrier_max(statistics.median(ts), world) / world
         mat_bytes = int(stats["n_tensor"]) * 2 * 64 * 64 * 4
+        med = np.median(np.array(profs), axis=0)
         e2e = {"value": e2e_ms, "unit": "ms/circuit", "h2d_bytes_per_step": int(ops.nbytes) + mat_bytes,
                "d2h_bytes_per_step": (1 << nq) * 8,
-               "note": "ketgpu_run: host ops in, 2^30 amplitudes out to a host complex128 buffer"}
+               "breakdown_ms": {"plan": med[0], "state_reset": med[1], "execute": med[2], "download": med[3],
+                                "download_copy_wait": med[4], "download_widen_own_share": med[5],
+                                "calls_ms": ts},
+               "host": {"cpu": host_cpu(), "threads": os.cpu_count()},
+               "note": "ketgpu_run: host ops in, 2^30 amplitudes out to a host complex128 buffer; "
+                       "breakdown = host wall time per phase (ketgpu_run_last_profile), median of the timed calls"}
         del out
 
+    # ket itself: one full ket::run of the same circuit on every host thread,
+    # timed as the CPU baseline; its complex128 state is the FP64 oracle for
+    # the accuracy of the timed complex64 state
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and nq == N_QUBITS and args.depth == DEPTH:
+    full_size = nq == N_QUBITS and args.depth == DEPTH
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and full_size:
         try:
-            cpu = cpu_baseline_reference(ops)
+            secs, threads, ket_state = ket_full_run(ops, keep_state=not args.no_checks)
+            cpu = {"value": secs * 1e3, "unit": "ms/circuit", "cores": threads, "kind": "reference",
+                   "sample": f"one full ket::run of the same 30-qubit depth-40 circuit (complex128) through "
+                             f"ket's public API (oracle/_ref/libket_ref.so built from ket's sources), "
+                             f"set_num_threads(0) = {threads} threads on {host_cpu()}, timed around the call"}
+            if ket_state is not None:
+                kst = ket.DeviceState(nq, "c128")
+                kst.from_numpy(ket_state)
+                del ket_state
+                step()  # the timed plan again: its state is bit-identical to every timed step
+                cmp = state.compare(kst)
+                checks.update({"max_abs_vs_ket": cmp["max_abs"], "fidelity_vs_ket": cmp["fidelity"],
+                               "fidelity_unnormalised_vs_ket": cmp["fidelity_unnormalised"],
+                               "oracle": "ket::run complex128 state of the same circuit"})
+                kst.close()
         except Exception as ex:  # the reference build may be absent
             cpu = {"value": None, "unit": "ms/circuit", "cores": None, "kind": "reference",
                    "sample": f"unavailable: {ex}"}

@@ -108,7 +108,10 @@ int ketgpu_state_create(int32_t n_qubits, int32_t precision, ketgpu_state** out)
 int ketgpu_state_destroy(ketgpu_state* s);
 int ketgpu_state_reset(ketgpu_state* s); /* |0...0> */
 int ketgpu_state_info(const ketgpu_state* s, int32_t* n_qubits, int32_t* precision);
-/* Device pointer of the amplitudes (float2 or double2 per amplitude). */
+/* Device pointer of the amplitudes (float2 or double2 per amplitude).  The
+ * call counts as a write (the caller may change amplitudes through the
+ * pointer), so the next ketgpu_sample rebuilds the sampling tree; call it
+ * again after writing through a pointer obtained earlier. */
 void* ketgpu_state_device_ptr(const ketgpu_state* s);
 /* Copy amplitudes [first, first+count) to a host complex128 buffer. */
 int ketgpu_state_download(const ketgpu_state* s, uint64_t first, uint64_t count,
@@ -167,6 +170,15 @@ int ketgpu_apply(ketgpu_state* s, const ketgpu_op* ops, uint64_t n_ops,
  * own state. */
 int ketgpu_run(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
                const ketgpu_options* opt, double* out_c128);
+/* Host wall time of the phases of the calling thread's last ketgpu_run, in
+ * milliseconds: out6 = {plan (validate + fusion + block matrices), state
+ * (reset of the kept state or a new allocation), execute (launch to the
+ * circuit's completion on the device), download (all 2^n amplitudes into
+ * the host complex128 buffer), of which copy wait (waiting on device-to-host
+ * copies) and widen (the calling thread's own share of the complex64 ->
+ * complex128 conversion)}.  Zeros before the first call.  No counterpart in
+ * ket (its run, simulator.cpp:554-558, has no phases to report). */
+int ketgpu_run_last_profile(double* out6);
 /* Free the device state that ketgpu_run keeps between calls (no-op when
  * there is none).  No counterpart in ket, whose run holds no device memory. */
 int ketgpu_release_cache(void);
@@ -192,8 +204,12 @@ int ketgpu_expval_sum(const ketgpu_state* s, const double* coeffs,
  * and freed underneath it.  No counterpart in ket (a variant of this
  * backend's own ketgpu_expval_sum).  It uses a fixed scratch array of
  * 608,256 bytes that every GPU loading the library holds until exit, shared
- * by all calls (calls overlapping on one GPU race on it); the first call on a
- * device looks the array up (make it before any stream capture).  At most
+ * by all calls on that GPU: calls that overlap on one GPU (other streams or
+ * threads at the same time) race on it.  The array and this call's kernels
+ * are looked up, and so loaded onto the device, when the first state is
+ * created there (ketgpu_state_create), which allocates anyway; the call
+ * itself allocates nothing.  It synchronises the state's stream and copies
+ * the per-term results to the host before returning.  At most
  * KETGPU_NOALLOC_MAX_TERMS terms; more returns KETGPU_ERR_INVALID. */
 #define KETGPU_NOALLOC_MAX_TERMS 256
 int ketgpu_expval_sum_noalloc(const ketgpu_state* s, const double* coeffs,
@@ -207,11 +223,25 @@ int ketgpu_expval_terms(const ketgpu_state* s, const char* const* paulis,
 /* The draws ket::measure consumes: uniform_real_distribution<double>(0,1)
  * on std::mt19937{seed}, `count` of them in order. */
 int ketgpu_uniforms_mt19937(uint32_t seed, uint64_t count, double* out);
-/* Born-rule draws for the given uniforms (host arrays), one FP64 CDF built
- * once over a fixed summation tree (segments of 32, carries folded
- * top-down), each draw the first index whose running sum exceeds u. */
+/* Born-rule draws for the given uniforms (host arrays) from one FP64 CDF
+ * over a fixed summation tree (segments of 32, carries folded top-down),
+ * each draw the first index whose running sum exceeds u.  The tree is kept
+ * with the state and rebuilt only after the amplitudes changed (any
+ * execute, apply, reset, upload, copy into the state, or
+ * ketgpu_state_device_ptr), so repeated draws from one state -- ket's
+ * StateVectorSimulation::sample, statevector.cpp:33-42, called once per
+ * shot -- cost one descent each. */
 int ketgpu_sample(const ketgpu_state* s, const double* uniforms, uint64_t count,
                   uint64_t* out_indices);
+/* `count` draws with the uniforms of std::mt19937{seed} +
+ * uniform_real_distribution<double>(0,1), in order: the many-shot form of
+ * ket::sample (measurement.hpp:26-28 evolves per shot; this draws every shot
+ * from one evolution, as the CLI's shot loop would, cli/commands.cpp:159-166). */
+int ketgpu_sample_seeded(const ketgpu_state* s, uint32_t seed, uint64_t count,
+                         uint64_t* out_indices);
+/* Sampling-tree builds since load (all states): a tree is built once per
+ * state version.  No counterpart in ket. */
+uint64_t ketgpu_sample_tree_builds(void);
 /* One draw from std::mt19937{seed} (measurement.cpp:12-21 with a seeded rng). */
 int ketgpu_measure(const ketgpu_state* s, uint32_t seed, uint64_t* out_index);
 

@@ -79,6 +79,7 @@ def _load():
         "ketgpu_plan_pass_info": ([vp, u64, ct.POINTER(i32), ct.POINTER(i32), ct.POINTER(i32), pd], ct.c_int),
         "ketgpu_plan_pass_qubits": ([vp, u64, ct.POINTER(i32), i32, ct.POINTER(i32)], ct.c_int),
         "ketgpu_release_cache": ([], ct.c_int),
+        "ketgpu_run_last_profile": ([vp], ct.c_int),
         "ketgpu_plan_pass_tc_form": ([vp, u64, ct.POINTER(i32), ct.POINTER(i32)], ct.c_int),
         "ketgpu_state_stream": ([vp], vp),
         "ketgpu_apply": ([vp, vp, u64, ct.POINTER(Options)], ct.c_int),
@@ -93,6 +94,8 @@ def _load():
         "ketgpu_uniforms_mt19937": ([u32, u64, vp], ct.c_int),
         "ketgpu_sample": ([vp, vp, u64, vp], ct.c_int),
         "ketgpu_measure": ([vp, u32, ct.POINTER(u64)], ct.c_int),
+        "ketgpu_sample_seeded": ([vp, u32, u64, vp], ct.c_int),
+        "ketgpu_sample_tree_builds": ([], u64),
         "ketgpu_adjoint": ([i32, vp, u64, vp, vp, u64, u64, vp, vp, u64, i32, i32, vp, vp], ct.c_int),
         "ketgpu_adjoint_ex": ([i32, vp, u64, vp, vp, u64, u64, vp, vp, u64, i32, i32, i32, vp, vp], ct.c_int),
         "ketgpu_adjoint_plan_describe": ([i32, vp, u64, vp, i32, vp, u64, vp], ct.c_int),

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <atomic>
 #include <barrier>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -264,7 +265,20 @@ int down_ring() {
 std::mutex g_stage_mu;
 void* g_stage = nullptr;
 
-void download(const State& s, uint64_t first, uint64_t count, double* out) {
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Where a complex64 download spends the calling thread's time: waiting for
+// device-to-host copies, and widening its share of each chunk.
+struct DownloadTimes {
+  double copy_wait_ms = 0.0, widen_ms = 0.0;
+};
+
+// Phase times of the calling thread's last ketgpu_run (ketgpu_run_last_profile).
+thread_local double t_run_profile[6] = {0, 0, 0, 0, 0, 0};
+
+void download(const State& s, uint64_t first, uint64_t count, double* out, DownloadTimes* times = nullptr) {
   if (s.precision == KETGPU_C128) {
     KB_CUDA(cudaMemcpyAsync(out, static_cast<const double2*>(s.amps) + first, count * 16,
                             cudaMemcpyDeviceToHost, s.stream));
@@ -315,13 +329,17 @@ void download(const State& s, uint64_t first, uint64_t count, double* out) {
   for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
   for (uint64_t c = 0; c < std::min<uint64_t>(ring - 1, nchunks); ++c) issue(c);
   for (uint64_t c = 0; c < nchunks; ++c) {
+    const auto w0 = std::chrono::steady_clock::now();
     if (err == cudaSuccess) {
       const cudaError_t e = cudaEventSynchronize(ev[c % ring]);
       if (e != cudaSuccess) err = e;
     }
+    if (times) times->copy_wait_ms += ms_since(w0);
     if (c + ring - 1 < nchunks && err == cudaSuccess) issue(c + ring - 1);
     sync.arrive_and_wait();
+    const auto s0 = std::chrono::steady_clock::now();
     slice(0, c);
+    if (times) times->widen_ms += ms_since(s0);
     sync.arrive_and_wait();
   }
   for (auto& x : th) x.join();
@@ -330,6 +348,7 @@ void download(const State& s, uint64_t first, uint64_t count, double* out) {
 }
 
 void upload(State& s, uint64_t first, uint64_t count, const double* in) {
+  s.touch();
   if (s.precision == KETGPU_C128) {
     KB_CUDA(cudaMemcpyAsync(static_cast<double2*>(s.amps) + first, in, count * 16, cudaMemcpyHostToDevice,
                             s.stream));
@@ -407,8 +426,10 @@ State* create_state(int n, int precision) {
     cudaStreamDestroy(st->stream);
     check_cuda(e, "cudaMalloc(state)");
   }
-  set_ground(*st);
-  return st.release();
+  std::unique_ptr<State, void (*)(State*)> guard_st(st.release(), destroy_state);
+  noalloc_prepare(guard_st->device);
+  set_ground(*guard_st);
+  return guard_st.release();
 }
 
 void destroy_state(State* s) {
@@ -417,6 +438,7 @@ void destroy_state(State* s) {
   cudaGetDevice(&prev);
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->tree) cudaFree(s->tree);
   if (s->amps) cudaFree(s->amps);
   if (s->stream) cudaStreamDestroy(s->stream);
   if (prev >= 0) cudaSetDevice(prev);
@@ -461,7 +483,13 @@ KB_API int ketgpu_state_info(const ketgpu_state* s, int32_t* n, int32_t* precisi
   });
 }
 
-KB_API void* ketgpu_state_device_ptr(const ketgpu_state* s) { return s ? as_state(s)->amps : nullptr; }
+// Handing out the pointer counts as a write: the caller may change the
+// amplitudes through it, so a cached sampling tree is not reused.
+KB_API void* ketgpu_state_device_ptr(const ketgpu_state* s) {
+  if (!s) return nullptr;
+  as_state(s)->touch();
+  return as_state(s)->amps;
+}
 
 KB_API int ketgpu_state_download(const ketgpu_state* s, uint64_t first, uint64_t count, double* out) {
   return guard([&] {
@@ -506,6 +534,7 @@ KB_API int ketgpu_state_copy(const ketgpu_state* src, ketgpu_state* dst) {
     State& b = *as_state(dst);
     need(a.n == b.n && a.precision == b.precision, "states differ in size or precision");
     DeviceGuard g(b.device);
+    b.touch();
     KB_CUDA(cudaStreamSynchronize(a.stream));
     KB_CUDA(cudaMemcpyAsync(b.amps, a.amps, a.dim() * a.amp_bytes(), cudaMemcpyDefault, b.stream));
     KB_CUDA(cudaStreamSynchronize(b.stream));
@@ -577,10 +606,14 @@ KB_API int ketgpu_run(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const ket
     need(out_c128 != nullptr, "out is null");
     need(ops != nullptr || n_ops == 0, "ops is null");
     if (n < 0 || n > 40) fail(KETGPU_ERR_INVALID, "n_qubits must be in [0, 40]");
+    const auto t0 = std::chrono::steady_clock::now();
+    std::fill(t_run_profile, t_run_profile + 6, 0.0);
     validate_ops(n, ops, n_ops);
     const PlanOptions o = resolve_options(opt);
     Plan plan;
     build_plan(plan, n, ops, n_ops, o);
+    const double plan_ms = ms_since(t0);
+    const auto t1 = std::chrono::steady_clock::now();
     State* kept = nullptr;
     {
       std::lock_guard<std::mutex> lk(g_run_mu);
@@ -596,11 +629,27 @@ KB_API int ketgpu_run(int32_t n, const ketgpu_op* ops, uint64_t n_ops, const ket
       destroy_state(kept);
       st.reset(create_state(n, o.precision));
     }
+    const double state_ms = ms_since(t1);
+    const auto t2 = std::chrono::steady_clock::now();
     execute(plan, *st);
-    download(*st, 0, st->dim(), out_c128);
+    KB_CUDA(cudaStreamSynchronize(st->stream));
+    const double exec_ms = ms_since(t2);
+    const auto t3 = std::chrono::steady_clock::now();
+    DownloadTimes dt;
+    download(*st, 0, st->dim(), out_c128, &dt);
+    const double down_ms = ms_since(t3);
     check_tc_flag();
+    const double prof[6] = {plan_ms, state_ms, exec_ms, down_ms, dt.copy_wait_ms, dt.widen_ms};
+    std::copy(prof, prof + 6, t_run_profile);
     std::lock_guard<std::mutex> lk(g_run_mu);  // keep it for the next call
     if (!g_run_state) g_run_state = st.release();
+  });
+}
+
+KB_API int ketgpu_run_last_profile(double* out6) {
+  return guard([&] {
+    need(out6 != nullptr, "out is null");
+    std::copy(t_run_profile, t_run_profile + 6, out6);
   });
 }
 
@@ -688,6 +737,21 @@ KB_API int ketgpu_sample(const ketgpu_state* s, const double* u, uint64_t count,
     sample_tree(*as_state(s), u, count, out);
   });
 }
+
+KB_API int ketgpu_sample_seeded(const ketgpu_state* s, uint32_t seed, uint64_t count, uint64_t* out) {
+  return guard([&] {
+    need(s != nullptr, "state is null");
+    need(out != nullptr || count == 0, "out is null");
+    std::vector<double> u(count);
+    std::mt19937 rng{seed};
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    for (uint64_t i = 0; i < count; ++i) u[i] = dist(rng);
+    DeviceGuard g(as_state(s)->device);
+    sample_tree(*as_state(s), u.data(), count, out);
+  });
+}
+
+KB_API uint64_t ketgpu_sample_tree_builds(void) { return sample_tree_builds(); }
 
 KB_API int ketgpu_measure(const ketgpu_state* s, uint32_t seed, uint64_t* out) {
   return guard([&] {

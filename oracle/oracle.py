@@ -54,6 +54,27 @@ def make_ops(gates):
     return ops
 
 
+def brickwork_ops(n, depth, seed, uniforms):
+    """The random U + CX brick wall as flat ops, for harnesses that drive ket
+    without the B200 package.  Every layer applies U(theta, phi, lambda) to
+    every qubit (angles uniform on [0, 2pi), three draws per qubit in (layer,
+    qubit, theta/phi/lambda) order from std::mt19937{seed}), then CX on pairs
+    (a, a+1) for a = layer mod 2, layer mod 2 + 2, ...  `uniforms(seed,
+    count)` supplies uniform_real_distribution<double>(0, 1) draws; scaling
+    by 2pi is exact for libstdc++'s (b - a) * u + a with a = 0."""
+    two_pi = 6.283185307179586
+    u = uniforms(seed, 3 * n * depth) * two_pi
+    gates = []
+    k = 0
+    for layer in range(depth):
+        for q in range(n):
+            gates.append(("U", (q,), (u[k], u[k + 1], u[k + 2])))
+            k += 3
+        for a in range(layer % 2, n - 1, 2):
+            gates.append(("CX", (a, a + 1)))
+    return make_ops(gates)
+
+
 def build_oracle():
     """Compile the C restatement (fast; gcc only)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
@@ -212,6 +233,8 @@ class Reference:
         L.ref_num_threads.restype = ct.c_uint
         L.ref_run.argtypes = [i32, vp, sz, vp]
         L.ref_run_timed.argtypes = [i32, vp, sz, vp, vp]
+        if hasattr(L, "ref_run_timed_state"):
+            L.ref_run_timed_state.argtypes = [i32, vp, sz, vp, vp]
         L.ref_run_with_probes.argtypes = [i32, vp, sz, vp, vp, sz, vp]
         L.ref_expval.argtypes = [i32, vp, ct.c_char_p, vp]
         L.ref_expval_sum.argtypes = [i32, vp, vp, vp, sz, vp]
@@ -251,6 +274,14 @@ class Reference:
         amps = np.zeros(2 << n, dtype=np.float64)
         self._check(self.L.ref_run(n, ops.ctypes.data, len(ops), amps.ctypes.data))
         return amps.view(np.complex128)
+
+    def run_timed_state(self, n, ops):
+        """(seconds of ket::run alone, the state it returned)."""
+        secs = np.zeros(1)
+        amps = np.empty(2 << n, dtype=np.float64)
+        self._check(self.L.ref_run_timed_state(n, ops.ctypes.data, len(ops), secs.ctypes.data,
+                                               amps.ctypes.data))
+        return float(secs[0]), amps.view(np.complex128)
 
     def run_timed(self, n, ops):
         secs = np.zeros(1)

@@ -152,6 +152,20 @@ SHIM_API int ref_run_timed(int n, const ko_op* ops, std::size_t nops,
   });
 }
 
+// ket::run, timed around the call only, with the returned state copied to
+// out (2 * 2^n doubles) after the clock stops.
+SHIM_API int ref_run_timed_state(int n, const ko_op* ops, std::size_t nops,
+                                 double* secs, double* out) {
+  return guard([&] {
+    const ket::Circuit c = build(n, ops, nops);
+    const auto t0 = std::chrono::steady_clock::now();
+    const ket::State s = ket::run(c);
+    const auto t1 = std::chrono::steady_clock::now();
+    *secs = std::chrono::duration<double>(t1 - t0).count();
+    from_state(s, out);
+  });
+}
+
 // ket::run_with_probes (simulator.hpp:24): final state plus each probe's state
 // (probes_out holds n_probes * 2 * 2^n doubles).
 SHIM_API int ref_run_with_probes(int n, const ko_op* ops, std::size_t nops,

@@ -288,3 +288,23 @@ def test_learned_mode_without_a_model_falls_back_to_greedy():
     a = ket.plan_stats(c, ket.make_options("c64", "greedy", 5, True))
     b = ket.plan_stats(c, ket.make_options("c64", "learned", 5, True))
     assert a["n_passes"] == b["n_passes"] and a["bytes"] == b["bytes"]
+
+
+def test_reference_harness_builds_the_bench_circuit(reference, oracle):
+    """The reference arm of the benchmark generates the 30-qubit brick wall
+    without the B200 package; it must be the circuit the B200 arm times."""
+    from oracle.oracle import brickwork_ops
+    from ket_b200.workloads import random_brickwork
+    for n, depth, seed in ((30, 40, 1234), (7, 5, 3)):
+        want = random_brickwork(n, depth, seed).to_ops()
+        for uni in (reference.uniforms, oracle.uniforms):
+            got = brickwork_ops(n, depth, seed, uni)
+            assert got.tobytes() == want.tobytes()
+
+
+def test_reference_timed_run_returns_kets_state(reference, oracle):
+    from oracle.oracle import brickwork_ops
+    ops = brickwork_ops(8, 6, 5, oracle.uniforms)
+    secs, st = reference.run_timed_state(8, ops)
+    assert secs >= 0.0
+    assert np.array_equal(st, reference.run(8, ops))
