@@ -178,6 +178,14 @@ class DeviceState:
         check(lib.ketgpu_sample(self._h, u.ctypes.data, len(u), out.ctypes.data))
         return out
 
+    def sample_seeded(self, seed: int, count: int) -> np.ndarray:
+        """`count` draws with the uniforms of std::mt19937{seed}, in order
+        (ketgpu_sample_seeded); the sampling tree is reused while the state
+        is unchanged."""
+        out = np.empty(count, dtype=np.uint64)
+        check(lib.ketgpu_sample_seeded(self._h, int(seed) & 0xFFFFFFFF, count, out.ctypes.data))
+        return out
+
     def torch_view(self):
         """Zero-copy torch tensor over the device amplitudes (complex)."""
         import torch
@@ -433,7 +441,7 @@ def sample_shots(circuit: Circuit, shots: int, seed: int = 0) -> np.ndarray:
     std::mt19937{seed} stream in order; returns shots x n_clbits."""
     d = run_device(circuit)
     try:
-        outcomes = d.sample(uniforms(seed, shots))
+        outcomes = d.sample_seeded(seed, shots)
     finally:
         d.close()
     meas = circuit.measurements()

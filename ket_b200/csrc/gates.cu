@@ -461,6 +461,7 @@ double Pass::bytes(int n, size_t amp) const {
 }
 
 void set_ground(const State& s) {
+  s.touch();
   KB_CUDA(cudaMemsetAsync(s.amps, 0, s.dim() * s.amp_bytes(), s.stream));
   if (s.precision == KETGPU_C64)
     set_one_kernel<float><<<1, 1, 0, s.stream>>>(static_cast<float2*>(s.amps));
@@ -471,6 +472,7 @@ void set_ground(const State& s) {
 }
 
 void launch_pass(const State& s, const Plan& plan, const Pass& p) {
+  s.touch();
   if (p.kind == PassKind::NormCapture) {
     norm_to_device(s, plan.d_norm + 2, plan.d_norm);
     return;

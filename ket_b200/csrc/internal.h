@@ -45,8 +45,16 @@ struct State {
   int device = 0;
   void* amps = nullptr;  // float2[2^n] or double2[2^n]
   cudaStream_t stream = nullptr;
+  // Bumped by every write the library makes to the amplitudes (touch()).
+  mutable uint64_t version = 0;
+  // The sampling tree (FP64 level sums with folded carries) of the state at
+  // tree_version, kept for the next draws; built by sample_tree on demand.
+  mutable double* tree = nullptr;
+  mutable uint64_t tree_doubles = 0;
+  mutable uint64_t tree_version = ~uint64_t{0};
   uint64_t dim() const { return uint64_t{1} << n; }
   size_t amp_bytes() const { return precision == KETGPU_C64 ? 8 : 16; }
+  void touch() const { ++version; }
 };
 
 // ---- passes ----------------------------------------------------------------
@@ -173,6 +181,10 @@ bool tc_supported(int k);
 void set_ground(const State& s);
 // Squared norm into a device scalar (partials: kNormBlocks doubles).
 void norm_to_device(const State& s, double* partials, double* out);
+// Look up (and so load) the no-allocation entry point's scratch array and
+// kernels on `device`, which must be current; once per device, at the first
+// state created there.
+void noalloc_prepare(int device);
 // Free the device state that ketgpu_run keeps between calls (if any).
 void release_run_state();
 // s *= sqrt(target[0] / current[0]), factor read on the device.
@@ -183,7 +195,11 @@ void compare_states(const State& a, const State& b, double out[5]);
 void expval_terms(const State& s, const std::vector<uint64_t>& flip,
                   const std::vector<uint64_t>& sign, const std::vector<int>& phase,
                   double* out);
+// Born-rule draws for host uniforms; builds the state's sampling tree only
+// when the amplitudes changed since the last build (State::version).
 void sample_tree(const State& s, const double* u, uint64_t count, uint64_t* out);
+// Number of sampling-tree builds since load (all states).
+uint64_t sample_tree_builds();
 
 // Pauli-string masks (observable.cpp:68-113); throws Error(INVALID).
 void pauli_masks(int n, const char* pauli, uint64_t& flip, uint64_t& sign, int& phase_q);

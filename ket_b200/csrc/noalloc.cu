@@ -16,9 +16,15 @@
 // race on it.  Nothing in it needs to start at zero: each call writes every
 // partial and every result it reads back.  In host code the array's name is
 // only a host-side stand-in, so the device address is looked up once per
-// device with cudaGetSymbolAddress (the first call on a device does this
-// set-up, with that device current; make that first call before capturing
-// any stream).
+// device with cudaGetSymbolAddress, with that device current.
+//
+// That set-up runs when the first state is created on a device
+// (noalloc_prepare, called from create_state), not in the entry point.
+// Under CUDA's lazy module loading (the default since CUDA 12.2) this
+// module, its scratch array and its kernels are placed on a device only
+// when first used, and placing them takes device memory.  Doing it at state
+// creation -- which allocates the state anyway -- leaves nothing for the
+// entry point itself to allocate.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -119,21 +125,32 @@ std::mutex g_na_mu;
 double* g_na_ptr[64] = {nullptr};
 
 // Device address of the scratch array on `device` (which must be current).
+// The first lookup on a device also loads this module's kernels there
+// (cudaFuncGetAttributes), so that a later launch places no code either.
 double* scratch_on(int device) {
   if (device < 0 || device >= 64) fail(KETGPU_ERR_INVALID, "expval_sum_noalloc: device index out of range");
   std::lock_guard<std::mutex> lk(g_na_mu);
   if (!g_na_ptr[device]) {
     void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess)
       fail(KETGPU_ERR_CUDA, std::string("expval_sum_noalloc: cudaGetSymbolAddress failed: ") +
                                 cudaGetErrorString(e));
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, na_partial<float2>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, na_partial<double2>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, na_finish);
+    if (e != cudaSuccess)
+      fail(KETGPU_ERR_CUDA, std::string("expval_sum_noalloc: loading its kernels failed: ") + cudaGetErrorString(e));
     g_na_ptr[device] = static_cast<double*>(p);
   }
   return g_na_ptr[device];
 }
 
 }  // namespace
+
+void noalloc_prepare(int device) { (void)scratch_on(device); }
+
 }  // namespace kb
 
 using namespace kb;

@@ -499,6 +499,10 @@ void expval_terms(const State& st, const std::vector<uint64_t>& flip, const std:
   KB_CUDA(cudaStreamSynchronize(st.stream));
 }
 
+std::atomic<uint64_t> g_tree_builds{0};
+
+uint64_t sample_tree_builds() { return g_tree_builds.load(); }
+
 void sample_tree(const State& st, const double* u, uint64_t count, uint64_t* out) {
   Levels lv{};
   lv.size[0] = st.dim();
@@ -510,13 +514,21 @@ void sample_tree(const State& st, const double* u, uint64_t count, uint64_t* out
     lv.off[lv.L] = total;
     total += lv.size[lv.L];
   }
+  // The tree lives with the state (1/31 of a complex128 state's size, 1/15
+  // of a complex64 one) and is rebuilt only after the amplitudes changed.
+  if (total && !st.tree) {
+    KB_CUDA(cudaMalloc(&st.tree, sizeof(double) * total));
+    st.tree_doubles = total;
+  }
   const size_t ubytes = sizeof(double) * count, obytes = sizeof(uint64_t) * count;
-  Scratch sc(sizeof(double) * total + ubytes + obytes + 64, st.stream);
-  double* buf = sc.as<double>();
-  double* d_u = buf + total;
+  Scratch sc(ubytes + obytes + 64, st.stream);
+  double* buf = st.tree;
+  double* d_u = sc.as<double>();
   uint64_t* d_out = reinterpret_cast<uint64_t*>(d_u + count);
   KB_CUDA(cudaMemcpyAsync(d_u, u, ubytes, cudaMemcpyHostToDevice, st.stream));
-  for (int l = 1; l <= lv.L; ++l) {
+  const bool build = total && st.tree_version != st.version;
+  if (build) g_tree_builds.fetch_add(1);
+  for (int l = 1; build && l <= lv.L; ++l) {
     const uint64_t nd = lv.size[l];
     const int blocks = grid_for(nd, kSegThreads);  // one warp -> 32 outputs
     if (l == 1) {
@@ -532,7 +544,7 @@ void sample_tree(const State& st, const double* u, uint64_t count, uint64_t* out
     }
     count_launch();
   }
-  if (lv.L >= 1) {
+  if (build) {
     top_fold<<<1, 1, 0, st.stream>>>(buf + lv.off[lv.L], lv.size[lv.L]);
     count_launch();
     for (int l = lv.L - 1; l >= 1; --l) {
@@ -553,6 +565,7 @@ void sample_tree(const State& st, const double* u, uint64_t count, uint64_t* out
     count_launch();
   }
   KB_CUDA(cudaGetLastError());
+  if (build) st.tree_version = st.version;
   KB_CUDA(cudaMemcpyAsync(out, d_out, obytes, cudaMemcpyDeviceToHost, st.stream));
   KB_CUDA(cudaStreamSynchronize(st.stream));
 }

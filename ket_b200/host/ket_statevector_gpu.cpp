@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -175,6 +176,8 @@ class GpuStateVectorSimulation final : public Simulation {
     check(ketgpu_expval(state_.h, pauli.c_str(), &out));
     return out;
   }
+  // Every term of a Pauli sum in one batched reduction over the kept state.
+  double expval_sum(const PauliSum& h) const { return pauli_sum_on(state_, h); }
 
  private:
   ketgpu_options opt_;
@@ -258,6 +261,10 @@ double expval(const Circuit& circuit, const std::string& pauli, Method method) {
 
 double expval(const Circuit& circuit, const PauliSum& hamiltonian, Method method) {
   const std::unique_ptr<Simulation> sim = simulate(circuit, method);
+  // On the GPU every term is reduced in one launch; the coefficient-weighted
+  // sum is still taken in term order (observable.cpp:97-106 loops the terms).
+  if (const auto* gpu = dynamic_cast<const GpuStateVectorSimulation*>(sim.get()))
+    return gpu->expval_sum(hamiltonian);
   double total = 0.0;
   for (const auto& [coeff, pauli] : hamiltonian) total += coeff * sim->expval(pauli);
   return total;
@@ -269,7 +276,81 @@ std::unique_ptr<Simulation> make_statevector_simulation(const Circuit& circuit) 
 }
 
 // ---- stepper.hpp -----------------------------------------------------------
-// One DAG node per step; the held host state is advanced on the GPU.
+// One DAG node per step, applied on the GPU.  ket's header makes
+// Stepper::state() an inline read of the host member state_, so the host
+// copy must be current after every step; what stays on the device is the
+// state the next step starts from.  The device copy of the Stepper that moved
+// last is kept (one at a time: ket's Stepper has no destructor of ours, so
+// this bounds what a destroyed Stepper can leave behind), tagged with its
+// address, its host buffer and position; a step that finds another tag
+// uploads state_ first.  Each step then costs its gates plus one download,
+// instead of an upload and a download.
+namespace {
+
+struct StepperDevice {
+  std::mutex mu;
+  const Stepper* owner = nullptr;
+  const void* host = nullptr;  // address of the owner's first amplitude when the copy was made
+  std::size_t pos = 0, n = 0;
+  std::unique_ptr<DeviceState> dev;
+};
+
+StepperDevice& stepper_device() {
+  static StepperDevice d;
+  return d;
+}
+
+std::vector<ketgpu_op> node_ops(const Circuit& c, std::size_t from, std::size_t to) {
+  std::vector<ketgpu_op> ops;
+  for (std::size_t i = from; i < to; ++i) {
+    const Gate& g = c.dag().nodes()[i].gate;
+    if (g.type == GateType::Measure || g.type == GateType::Barrier || g.type == GateType::Probe) continue;
+    if (g.type == GateType::Composite) {
+      std::vector<std::size_t> sub(g.definition->n_qubits());
+      for (std::size_t j = 0; j < g.qubits.size(); ++j) sub[j] = g.qubits[j].index;
+      flatten(*g.definition, sub, ops, nullptr);
+    } else {
+      ketgpu_op op{};
+      op.type = static_cast<int32_t>(g.type);
+      op.nq = static_cast<int32_t>(g.qubits.size());
+      for (std::size_t j = 0; j < g.qubits.size() && j < 3; ++j) op.q[j] = static_cast<int32_t>(g.qubits[j].index);
+      for (std::size_t j = 0; j < g.params.size() && j < 3; ++j) op.p[j] = g.params[j];
+      ops.push_back(op);
+    }
+  }
+  return ops;
+}
+
+// Apply DAG nodes [from, to) of `c` to `state` (the Stepper `who` at
+// position `from`), leaving the result in `state` and on the device.
+void advance(const Stepper* who, State& state, const Circuit& c, std::size_t from, std::size_t to) {
+  const std::vector<ketgpu_op> ops = node_ops(c, from, to);
+  StepperDevice& sd = stepper_device();
+  std::lock_guard<std::mutex> lk(sd.mu);
+  const bool mine = sd.dev && sd.owner == who && sd.host == static_cast<const void*>(&state[0]) && sd.pos == from &&
+                    sd.n == c.n_qubits();
+  if (ops.empty()) {  // structural nodes only: the state does not change
+    if (mine) sd.pos = to;
+    return;
+  }
+  if (!mine) {
+    sd.owner = nullptr;
+    sd.dev.reset();
+    sd.dev = DeviceState::from_host(state);
+  }
+  ketgpu_options o = options();
+  o.precision = KETGPU_C128;
+  o.fusion = KETGPU_FUSE_NONE;  // the stepper's semantics: one node at a time
+  sd.dev->apply(ops, o);
+  check(ketgpu_state_download(sd.dev->h, 0, state.size(), reinterpret_cast<double*>(&state[0])));
+  sd.owner = who;
+  sd.host = &state[0];
+  sd.pos = to;
+  sd.n = c.n_qubits();
+}
+
+}  // namespace
+
 Stepper::Stepper(Circuit circuit)
     : circuit_(std::move(circuit)),
       state_(ground(circuit_.n_qubits())),
@@ -281,40 +362,9 @@ void Stepper::reset() {
   pos_ = 0;
 }
 
-namespace {
-void advance(State& state, const Circuit& c, std::size_t from, std::size_t to) {
-  std::vector<ketgpu_op> ops;
-  for (std::size_t i = from; i < to; ++i) {
-    const Gate& g = c.dag().nodes()[i].gate;
-    if (g.type == GateType::Measure || g.type == GateType::Barrier || g.type == GateType::Probe) continue;
-    std::vector<ketgpu_op> tmp;
-    if (g.type == GateType::Composite) {
-      std::vector<std::size_t> sub(g.definition->n_qubits());
-      for (std::size_t j = 0; j < g.qubits.size(); ++j) sub[j] = g.qubits[j].index;
-      flatten(*g.definition, sub, tmp, nullptr);
-    } else {
-      ketgpu_op op{};
-      op.type = static_cast<int32_t>(g.type);
-      op.nq = static_cast<int32_t>(g.qubits.size());
-      for (std::size_t j = 0; j < g.qubits.size() && j < 3; ++j) op.q[j] = static_cast<int32_t>(g.qubits[j].index);
-      for (std::size_t j = 0; j < g.params.size() && j < 3; ++j) op.p[j] = g.params[j];
-      tmp.push_back(op);
-    }
-    ops.insert(ops.end(), tmp.begin(), tmp.end());
-  }
-  if (ops.empty()) return;
-  auto d = DeviceState::from_host(state);
-  ketgpu_options o = options();
-  o.precision = KETGPU_C128;
-  o.fusion = KETGPU_FUSE_NONE;  // the stepper's semantics: one node at a time
-  d->apply(ops, o);
-  state = d->to_host(c.n_qubits());
-}
-}  // namespace
-
 bool Stepper::step() {
   if (pos_ >= n_steps_) return false;
-  advance(state_, circuit_, pos_, pos_ + 1);
+  advance(this, state_, circuit_, pos_, pos_ + 1);
   ++pos_;
   return true;
 }
@@ -322,7 +372,7 @@ bool Stepper::step() {
 void Stepper::seek(std::size_t step) {
   if (step > n_steps_) step = n_steps_;
   if (step < pos_) reset();
-  advance(state_, circuit_, pos_, step);
+  advance(this, state_, circuit_, pos_, step);
   pos_ = step;
 }
 

@@ -197,7 +197,7 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     ap.add_argument("--check", type=int, default=60, help="held-out circuits whose states are compared")
     ap.add_argument("--unfused", type=int, default=60, help="held-out circuits also timed unfused")
     ap.add_argument("--steps", type=int, default=4000)
-    ap.add_argument("--out", default="gpurun_out/planner.json")
+    ap.add_argument("--out", required=True, help="JSON file for the training and evaluation record")
     ap.add_argument("--save", default=DEFAULT_MODEL)
     ap.add_argument("--nmax", type=int, default=32)
     ap.add_argument("--load", default=None, help="evaluate this trained model (skips measuring and training)")

@@ -183,3 +183,31 @@ def test_stabilizer_equals_gpu_statevector_on_cliffords():
             stab = D.expval_circuit(n, ops, [(1.0, p)], method=2)
             sv = D.expval_circuit(n, ops, [(1.0, p)], method=1)
             assert abs(stab - sv) < 1e-9, (seed, p)
+
+
+@pytest.mark.gpu
+def test_simulation_sample_draws_from_one_tree(oracle):
+    """ket's StateVectorSimulation::sample (statevector.cpp:33-42), called once
+    per shot as ket's CLI does (cli/commands.cpp:159-166): 10^4 draws on a
+    5-qubit register are ket's own draws bit for bit (one 32-amplitude
+    segment: the tree is ket's scan), and on 12 qubits every draw comes from
+    one sampling tree built once for the state, equal to the oracle's tree
+    sampler fed the same std::mt19937 stream."""
+    from ket_b200 import _lib
+    R, D = _libs()
+    n = 5
+    ops = np.concatenate([_random_ops(n, 60, 31), make_ops([("Measure", [q, q]) for q in range(n)])])
+    a, _ = R.sample(n, ops, 77, 10000, method=1, evolve_once=True)
+    b, _ = D.sample(n, ops, 77, 10000, method=1, evolve_once=True)
+    assert np.array_equal(a, b)
+
+    n = 12
+    body = _random_ops(n, 150, 32)
+    ops = np.concatenate([body, make_ops([("Measure", [q, q]) for q in range(n)])])
+    builds = _lib.lib.ketgpu_sample_tree_builds()
+    got, _ = D.sample(n, ops, 78, 10000, method=1, evolve_once=True)
+    assert _lib.lib.ketgpu_sample_tree_builds() - builds == 1
+    st = D.run(n, body)
+    idx = oracle.sample_tree(n, st, oracle.uniforms(78, 10000))
+    want = ((idx[:, None] >> np.arange(n, dtype=np.uint64)) & np.uint64(1)).astype(np.int32)
+    assert np.array_equal(got, want)
