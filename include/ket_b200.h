@@ -66,7 +66,9 @@ typedef struct ketgpu_op {
 enum ketgpu_precision { KETGPU_C64 = 0, KETGPU_C128 = 1 };
 
 enum ketgpu_fusion {
-  KETGPU_FUSE_NONE = 0,      /* one kernel per gate (the plain method) */
+  KETGPU_FUSE_NONE = 0,      /* the plain method: one kernel per gate, except
+                                consecutive gates on qubits 0..10 share one
+                                pass over chunks staged in shared memory */
   KETGPU_FUSE_REFERENCE = 1, /* ket's own block rule (simulator.cpp:400-477) */
   KETGPU_FUSE_GREEDY = 2,    /* DAG-aware k-qubit blocks, static cost model */
   KETGPU_FUSE_LEARNED = 3    /* k-qubit blocks scored by the MLP cost model */
@@ -137,8 +139,9 @@ int ketgpu_plan_execute(const ketgpu_plan* p, ketgpu_state* s);
  * pass_ms receives n_passes durations (milliseconds).  Synchronises. */
 int ketgpu_plan_execute_timed(const ketgpu_plan* p, ketgpu_state* s, float* pass_ms);
 /* Describe pass `index`: kind (0 pair, 1 phase, 2 dense block, 3 norm
- * capture/restore, 4 diagonal run), qubits k (block qubits, or the qubits a
- * diagonal run touches), tensor-core flag and algorithmic HBM bytes. */
+ * capture/restore, 4 diagonal run, 5 shared-memory run of low-qubit gates),
+ * k (block qubits, the qubits a diagonal run touches, or a shared-memory
+ * run's gate count), tensor-core flag and algorithmic HBM bytes. */
 int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* kind, int32_t* k,
                           int32_t* tensor, double* bytes);
 /* The qubits pass `index` acts on, ascending: a dense block's qubits (matrix

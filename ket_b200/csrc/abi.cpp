@@ -61,6 +61,7 @@ Plan::~Plan() {
     if (d_tc) cudaFree(d_tc);
     if (d_norm) cudaFree(d_norm);
     if (d_diag) cudaFree(d_diag);
+    if (d_runs) cudaFree(d_runs);
     if (prev >= 0) cudaSetDevice(prev);
   }
 }
@@ -106,6 +107,18 @@ void upload_plan_matrices(Plan& plan, int device) {
     }
     KB_CUDA(cudaMalloc(&plan.d_diag, all.size()));
     KB_CUDA(cudaMemcpy(plan.d_diag, all.data(), all.size(), cudaMemcpyHostToDevice));
+  }
+  if (!plan.runs.empty()) {
+    std::vector<unsigned char> all, one;
+    plan.offrun.assign(plan.runs.size(), 0);
+    for (size_t i = 0; i < plan.runs.size(); ++i) {
+      run_device_data(plan.runs[i], plan.precision, one);
+      plan.offrun[i] = all.size();
+      all.insert(all.end(), one.begin(), one.end());
+      while (all.size() % 256) all.push_back(0);
+    }
+    KB_CUDA(cudaMalloc(&plan.d_runs, all.size()));
+    KB_CUDA(cudaMemcpy(plan.d_runs, all.data(), all.size(), cudaMemcpyHostToDevice));
   }
   if (plan.matrices.empty()) return;
   std::vector<double> h64;
@@ -795,12 +808,16 @@ KB_API int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* 
     if (index >= plan.passes.size()) fail(KETGPU_ERR_OUT_OF_RANGE, "pass index out of range");
     const Pass& ps = plan.passes[index];
     if (kind)
-      *kind = ps.kind == PassKind::Pair       ? 0
-              : ps.kind == PassKind::Phase    ? 1
-              : ps.kind == PassKind::Fused    ? 2
-              : ps.kind == PassKind::Diagonal ? 4
-                                              : 3;
-    if (k) *k = (ps.kind == PassKind::Fused || ps.kind == PassKind::Diagonal) ? ps.k : ps.nfixed;
+      *kind = ps.kind == PassKind::Pair        ? 0
+              : ps.kind == PassKind::Phase     ? 1
+              : ps.kind == PassKind::Fused     ? 2
+              : ps.kind == PassKind::Diagonal  ? 4
+              : ps.kind == PassKind::SharedRun ? 5
+                                               : 3;
+    if (k)
+      *k = (ps.kind == PassKind::Fused || ps.kind == PassKind::Diagonal) ? ps.k
+           : ps.kind == PassKind::SharedRun                              ? ps.n_gates
+                                                                         : ps.nfixed;
     if (tensor) *tensor = ps.tensor ? 1 : 0;
     if (bytes) *bytes = ps.bytes(plan.n, plan.precision == KETGPU_C64 ? 8 : 16);
   });

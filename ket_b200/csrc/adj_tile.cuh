@@ -330,11 +330,13 @@ __device__ __forceinline__ float pk_dispatch(int op, PackState& a, PackState& l,
 // generated with their phases and gates as compile-time constants.
 
 // Per-CTA set-up: tile offset tables, the block's gate records and this
-// set's packed coefficients (U forward, U^dag reverse), zeroed gradient sums.
+// set's packed coefficients (U forward, U^dag reverse), and `acc_words`
+// zeroed 4-byte words of gradient sums.
 template <bool REV>
 __device__ __forceinline__ void c64_setup(const TileGeom& tg, const TGate* __restrict__ gates, int ngates,
-                                          const float* __restrict__ mats, uint64_t mat_stride, int set, int ngrad,
-                                          uint64_t* off_lo, uint64_t* off_hi, f2* spk, double* acc) {
+                                          const float* __restrict__ mats, uint64_t mat_stride, int set,
+                                          int acc_words, uint64_t* off_lo, uint64_t* off_hi, f2* spk,
+                                          float* acc) {
   constexpr int TB = TileCfg<float>::TB;
   const int tid = threadIdx.x;
   if (tid < 128) {
@@ -369,7 +371,7 @@ __device__ __forceinline__ void c64_setup(const TileGeom& tg, const TGate* __res
     c[15] = 0;
   }
   if (REV)
-    for (int i = tid; i < kTileWarps * ngrad; i += kTileThreads) acc[i] = 0.0;
+    for (int i = tid; i < acc_words; i += kTileThreads) acc[i] = 0.f;
 }
 
 __device__ __forceinline__ uint64_t c64_tile_base(const TileGeom& tg, uint64_t t) {
@@ -464,6 +466,22 @@ __device__ __forceinline__ void c64_flush(const double* acc, int ngrad, double* 
   for (int g = threadIdx.x; g < ngrad; g += kTileThreads) {
     double v = 0.0;
     for (int w = 0; w < kTileWarps; ++w) v += acc[w * ngrad + g];
+    partial[((uint64_t)set * ngrad + g) * gridDim.x + blockIdx.x] = v;
+  }
+}
+
+// Blocks with few gradients: each thread sums its own gradient terms over
+// all of its tiles in FP32, in shared-memory slots of stride GS (odd, so a
+// warp's slots fall in distinct banks), with no per-tile warp reduction.
+// The CTA folds the slots in FP64, in thread order, once at its end.
+__device__ __forceinline__ void c64_grad_slot(float* accf, int gs, int slot, float part) {
+  accf[threadIdx.x * gs + slot] += part;
+}
+
+__device__ __forceinline__ void c64_flush_slots(const float* accf, int gs, int ngrad, double* partial, int set) {
+  for (int g = threadIdx.x; g < ngrad; g += kTileThreads) {
+    double v = 0.0;
+    for (int t = 0; t < kTileThreads; ++t) v += (double)accf[t * gs + g];
     partial[((uint64_t)set * ngrad + g) * gridDim.x + blockIdx.x] = v;
   }
 }

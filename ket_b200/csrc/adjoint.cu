@@ -1306,9 +1306,20 @@ int pk_opcode_host(const TGate& g, bool rev) {
 
 // The kernel of one complex64 block: phases (in sweep order) and their gates
 // as constants.  Parameters as tile_sweep_c64, without the phase table.
+// Gradient slots per thread for a reverse block with `ngrad` gradients: the
+// odd stride of the per-thread FP32 sums, or 0 for the per-tile warp
+// reduction into per-warp FP64 sums (blocks with many gradients, whose
+// per-thread slots would not leave room for two CTAs per SM).
+constexpr int kThreadGradMax = 31;
+int grad_slot_stride(int ngrad) { return ngrad > 0 && ngrad <= kThreadGradMax ? (ngrad | 1) : 0; }
+
 std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGate>& gates, bool rev) {
   std::string o;
   auto line = [&](const std::string& x) { o += x + "\n"; };
+  int ngrad_block = 0;
+  for (const TGate& g : gates)
+    if (g.grad >= 0) ngrad_block = std::max(ngrad_block, (int)g.grad + 1);
+  const int gs = rev ? grad_slot_stride(ngrad_block) : 0;
   // Reverse: two CTAs per SM with one tile buffer each (load, compute,
   // store) beat one CTA with two buffers: the other CTA's work covers the
   // loads.  Forward: two CTAs, each prefetching its next tile.
@@ -1323,13 +1334,16 @@ std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGat
   line("  extern __shared__ __align__(16) unsigned char tsm[];");
   line("  float2* bufs = reinterpret_cast<float2*>(tsm);");
   line("  f2* spk = reinterpret_cast<f2*>(tsm + (SINGLE ? 1 : 2) * BUF * sizeof(float2));");
-  line("  double* acc = reinterpret_cast<double*>(spk + 16 * ngates);");
+  line("  float* accf = reinterpret_cast<float*>(spk + 16 * ngates);");
+  line("  double* acc = reinterpret_cast<double*>(accf);");
+  line("  constexpr int GS = " + std::to_string(gs) + ";  // per-thread gradient slots (0: per-warp sums)");
   line("  __shared__ uint64_t off_lo[64], off_hi[64];");
   line("  const int tid = threadIdx.x;");
   line("  const int set = blockIdx.y;");
   line("  float2* s = psi + (uint64_t)set * dim;");
   line("  float2* l = REV ? lam + (uint64_t)set * dim : nullptr;");
-  line("  c64_setup<REV>(tg, gates, ngates, mats, mat_stride, set, ngrad, off_lo, off_hi, spk, acc);");
+  line("  c64_setup<REV>(tg, gates, ngates, mats, mat_stride, set, GS ? kTileThreads * GS : 2 * kTileWarps * ngrad,");
+  line("                 off_lo, off_hi, spk, accf);");
   line("  __syncthreads();");
   line("  int cur = 0;");
   line("  if (!SINGLE && blockIdx.x < tg.n_tiles) c64_prefetch<REV>(tg, off_lo, off_hi, blockIdx.x, bufs, s, l);");
@@ -1375,7 +1389,10 @@ std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGat
       if (g.cm_g) line("        if ((gbase & " + std::to_string((int)g.cm_g) + ") == " + std::to_string((int)g.cm_g) +
                        ") " + call);
       else line("        " + call);
-      if (rev && g.grad >= 0) line("        c64_grad(acc, ngrad, " + std::to_string((int)g.grad) + ", part);");
+      if (rev && g.grad >= 0) {
+        if (gs) line("        c64_grad_slot(accf, GS, " + std::to_string((int)g.grad) + ", part);");
+        else line("        c64_grad(acc, ngrad, " + std::to_string((int)g.grad) + ", part);");
+      }
       line("        (void)part; }");
     }
     line("      c64_store_phase<REV>(sp, sl, pg" + pb + ", A, L);");
@@ -1387,15 +1404,18 @@ std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGat
   line("    cur ^= 1;");
   line("  }");
   line("  asm volatile(\"cp.async.wait_all;\\n\" ::: \"memory\");");
-  line("  if (REV) c64_flush(acc, ngrad, partial, set);");
+  if (gs) line("  __syncthreads();");
+  line(gs ? "  c64_flush_slots(accf, GS, ngrad, partial, set);" : "  if (REV) c64_flush(acc, ngrad, partial, set);");
   line("}");
   return o;
 }
 
 size_t jit_smem(bool rev, int ngates, int ngrad) {
-  // forward: two buffers of psi; reverse: one buffer of psi and lambda
-  return 2 * (size_t{1} << TileCfg<float>::TB) * sizeof(float2) + (size_t)ngates * 16 * sizeof(f2) +
-         (rev ? (size_t)kTileWarps * ngrad * 8 : 0);
+  // forward: two buffers of psi; reverse: one buffer of psi and lambda, and
+  // the gradient sums (per-thread FP32 slots or per-warp FP64)
+  const int gs = grad_slot_stride(ngrad);
+  const size_t acc = !rev ? 0 : gs ? (size_t)kTileThreads * gs * 4 : (size_t)kTileWarps * ngrad * 8;
+  return 2 * (size_t{1} << TileCfg<float>::TB) * sizeof(float2) + (size_t)ngates * 16 * sizeof(f2) + acc;
 }
 
 // Dynamic shared memory of one tiled sweep launch (see the kernels).
@@ -1630,12 +1650,20 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
         if (jit_rev[bi])
           KB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(jit_rev[bi]),
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)jit_smem(true, kMaxBlockGates, kMaxBlockGrads)));
+                                       (int)std::max(jit_smem(true, kMaxBlockGates, kMaxBlockGrads),
+                                                     jit_smem(true, kMaxBlockGates, kThreadGradMax))));
       }
     }
     const uint64_t n_tiles = uint64_t{1} << (n - TB);
-    // one CTA per SM: about 4 waves of 148 CTAs over the chunk's sets
-    gx = (int)std::min<uint64_t>(n_tiles, std::max<uint64_t>(1, (148ull * 4 + chunk - 1) / chunk));
+    // About eight rounds of every resident CTA (two per SM) over the chunk's
+    // sets, in whole rounds where the set count allows: a grid of 10 x 64
+    // CTAs on 296 slots ran two full rounds and a third of 48 CTAs, leaving
+    // most SMs idle for a third of each sweep.
+    int sms = 148, dev = 0;
+    KB_CUDA(cudaGetDevice(&dev));
+    KB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const uint64_t slots = 2ull * (uint64_t)sms;
+    gx = (int)std::min<uint64_t>(n_tiles, std::max<uint64_t>(1, (8 * slots + chunk / 2) / chunk));
     for (TBlock& b : tp.blocks) {
       b.part_off = grad_doubles;
       grad_doubles += b.grad_gate.size() * chunk * (size_t)gx;

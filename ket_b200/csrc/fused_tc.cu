@@ -1,7 +1,7 @@
 // fused_tc.cu -- dense k-qubit block apply on the 5th-generation tensor cores.
 //
 // The sm_100a replacement for ket's apply_matrix (src/simulator.cpp:357-393)
-// when the fusion planner hands it a 2^k x 2^k complex block (k = 4 or 5) and
+// when the fusion planner hands it a 2^k x 2^k complex block (k = 4, 5 or 6) and
 // the state is complex64.
 //
 // Formulation.  A tile is 128 groups x 2^k target combinations; group g's
@@ -56,17 +56,26 @@ struct TcCfg {
   static constexpr int RAW_BYTES = TILE * 8;  // one staging image (= one A image)
   static constexpr int B_BYTES = N * K * 4;   // one B image
   static constexpr int KSTEPS = K / 8;        // tf32 MMA K = 8
-  // tensor memory: per tile parity an A region (hi | lo, 2K columns) and an
-  // accumulator region (main | correction, 2N columns)
+  // Tensor memory: A regions (hi | lo, 2K columns) and two accumulator
+  // regions (main | correction).  k <= 5: two A regions (tile parity) and one
+  // MMA pass of N columns per tile.  k = 6 (SPLIT): 2K + 2 * 2N would need
+  // 1024 columns, so one A region and two passes of N/2 columns per tile,
+  // each into its own accumulator region: the epilogue drains the first half
+  // while the second half's MMAs run, and the next tile's split waits only
+  // for this tile's MMAs.
+  static constexpr bool SPLIT = KQ == 6;
+  static constexpr int PASSES = SPLIT ? 2 : 1;
+  static constexpr int NH = N / PASSES;  // accumulator columns of one MMA pass
+  static constexpr int A_BUFS = SPLIT ? 1 : 2;
   static constexpr int A_COLS = 2 * K;
-  static constexpr int ACC_COLS = 2 * N;
-  static constexpr int TMEM_COLS = 2 * A_COLS + 2 * ACC_COLS;
+  static constexpr int ACC_COLS = 2 * NH;
+  static constexpr int TMEM_COLS = A_BUFS * A_COLS + 2 * ACC_COLS;
   // staging images: as many as fit next to the B images (loads in flight)
   static constexpr int SLOTS_FIT = (kSmemBudget - 1024 - 2 * B_BYTES) / RAW_BYTES;
   static constexpr int SLOTS = SLOTS_FIT > 12 ? 12 : SLOTS_FIT;
   static constexpr size_t SMEM = (size_t)SLOTS * RAW_BYTES + 2 * B_BYTES + 1024;  // + alignment slack
-  static_assert(TMEM_COLS <= 512, "tensor memory budget");
-  static_assert(SLOTS >= 3, "shared memory budget");
+  static_assert(TMEM_COLS <= 512 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory budget");
+  static_assert(SLOTS >= (SPLIT ? 1 : 3), "shared memory budget");
 };
 
 struct TcGeom {
@@ -83,8 +92,8 @@ struct TcGeom {
   int tma_dims;
   int tma_start[5];
   uint64_t tma_mask[5];
-  uint32_t ctile[32];
-  uint64_t cdep[32];  // offset of target combination c from its group's amplitude
+  uint32_t ctile[64];
+  uint64_t cdep[64];  // offset of target combination c from its group's amplitude
   uint64_t n_tiles;
 };
 
@@ -218,6 +227,7 @@ __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.
 // both K-major, N>>3 at [17,23), M>>4 at [24,29).
 template <int N>
 __host__ __device__ constexpr uint32_t tf32_idesc() {
+  static_assert(N % 16 == 0 && N >= 16 && N <= 256, "M = 128 needs N a multiple of 16 in [16, 256]");
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
@@ -445,10 +455,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     for (uint64_t j = 0; j < count; ++j) {
       const int slot = (int)(j % S);
       if (!wait(&bar_full[slot], (uint32_t)((j / S) & 1))) break;
-      if (j >= 2 && !wait(&bar_mma[j & 1], (uint32_t)(((j - 2) >> 1) & 1))) break;
+      // the A region is free once the MMAs that read it last have completed:
+      // tile j-2's (two regions), or tile j-1's second pass (one region)
+      if constexpr (Cfg::SPLIT) {
+        if (j >= 1 && !wait(&bar_mma[1], (uint32_t)((j - 1) & 1))) break;
+      } else {
+        if (j >= 2 && !wait(&bar_mma[j & 1], (uint32_t)(((j - 2) >> 1) & 1))) break;
+      }
       tc_fence_after();
       const unsigned char* img = raw + slot * Cfg::RAW_BYTES;
-      const uint32_t areg = tmem + lane_off + (uint32_t)((j & 1) * Cfg::A_COLS);
+      const uint32_t areg = tmem + lane_off + (uint32_t)((j % Cfg::A_BUFS) * Cfg::A_COLS);
 #pragma unroll
       for (int part = 0; part < K / 16; ++part) {
         uint32_t hi[16], lo[16];
@@ -485,7 +501,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
       asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       tc_fence_before();
-      arrive(&bar_a_ready[j & 1]);
+      arrive(&bar_a_ready[j % Cfg::A_BUFS]);
       if (g.direct) arrive(&bar_free[slot]);  // nothing else reads this image
     }
   } else if (warp < 12) {
@@ -503,55 +519,73 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           if ((row >> gb) & 1) gdep |= uint64_t{1} << g.tile_pos[jb];
           ++gb;
         }
-      for (uint64_t j = 0; j < count; ++j) {
-        if (!wait(&bar_mma[j & 1], (uint32_t)((j >> 1) & 1))) break;
-        tc_fence_after();
-        const uint32_t acc = tmem + (uint32_t)(2 * Cfg::A_COLS + (j & 1) * Cfg::ACC_COLS) + ((uint32_t)(32 * q) << 16);
+      bool ok = true;
+      for (uint64_t j = 0; j < count && ok; ++j) {
         float2* dst = s + base_ring[j % (2 * S)] + gdep;
+        for (int h = 0; h < Cfg::PASSES; ++h) {
+          const uint64_t u = j * Cfg::PASSES + h;  // accumulator use: region u%2, its (u/2)-th
+          if (!wait(&bar_mma[u & 1], (uint32_t)((u >> 1) & 1))) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS) +
+                               ((uint32_t)(32 * q) << 16);
 #pragma unroll
-        for (int part = 0; part < N / 16; ++part) {
-          float vm[16], vc[16];
-          tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
-          tmem_ld<16>(acc + (uint32_t)(N + part * 16), vc);
-          tmem_ld_wait();
+          for (int part = 0; part < Cfg::NH / 16; ++part) {
+            float vm[16], vc[16];
+            tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
+            tmem_ld<16>(acc + (uint32_t)(Cfg::NH + part * 16), vc);
+            tmem_ld_wait();
 #pragma unroll
-          for (int i = 0; i < 8; ++i)
-            dst[g.cdep[part * 8 + i]] = make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
+            for (int i = 0; i < 8; ++i)
+              dst[g.cdep[h * (Cfg::NH / 2) + part * 8 + i]] =
+                  make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
+          }
+          tc_fence_before();
+          arrive(&bar_acc_free[u & 1]);
         }
-        tc_fence_before();
-        arrive(&bar_acc_free[j & 1]);
       }
     } else {
     uint64_t goff[CPT];
     uint32_t soff[CPT];
     chunk_offsets(t, goff, soff, true);
-    for (uint64_t j = 0; j < count; ++j) {
+    bool ok = true;
+    for (uint64_t j = 0; j < count && ok; ++j) {
       const int slot = (int)(j % S);
-      if (!wait(&bar_mma[j & 1], (uint32_t)((j >> 1) & 1))) break;
-      tc_fence_after();
       unsigned char* out = raw + slot * Cfg::RAW_BYTES;
-      const uint32_t acc = tmem + (uint32_t)(2 * Cfg::A_COLS + (j & 1) * Cfg::ACC_COLS) + ((uint32_t)(32 * q) << 16);
-#pragma unroll
-      for (int part = 0; part < N / 16; ++part) {
-        float vm[16], vc[16];
-        tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
-        tmem_ld<16>(acc + (uint32_t)(N + part * 16), vc);
-        tmem_ld_wait();
-        if (q0_group) {
-#pragma unroll
-          for (int i = 0; i < 8; ++i)
-            *reinterpret_cast<float2*>(out + pair_slot(row, part * 8 + i)) =
-                make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
-        } else {
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            *reinterpret_cast<float4*>(out + sw128_offset(row, part * 16 + 4 * i, 128)) =
-                make_float4(vm[4 * i] + vc[4 * i], vm[4 * i + 1] + vc[4 * i + 1], vm[4 * i + 2] + vc[4 * i + 2],
-                            vm[4 * i + 3] + vc[4 * i + 3]);
+      for (int h = 0; h < Cfg::PASSES; ++h) {
+        const uint64_t u = j * Cfg::PASSES + h;
+        if (!wait(&bar_mma[u & 1], (uint32_t)((u >> 1) & 1))) {
+          ok = false;
+          break;
         }
+        tc_fence_after();
+        const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS) +
+                             ((uint32_t)(32 * q) << 16);
+#pragma unroll
+        for (int part = 0; part < Cfg::NH / 16; ++part) {
+          float vm[16], vc[16];
+          tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
+          tmem_ld<16>(acc + (uint32_t)(Cfg::NH + part * 16), vc);
+          tmem_ld_wait();
+          if (q0_group) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+              *reinterpret_cast<float2*>(out + pair_slot(row, h * (Cfg::NH / 2) + part * 8 + i)) =
+                  make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              *reinterpret_cast<float4*>(out + sw128_offset(row, h * Cfg::NH + part * 16 + 4 * i, 128)) =
+                  make_float4(vm[4 * i] + vc[4 * i], vm[4 * i + 1] + vc[4 * i + 1], vm[4 * i + 2] + vc[4 * i + 2],
+                              vm[4 * i + 3] + vc[4 * i + 3]);
+          }
+        }
+        tc_fence_before();
+        arrive(&bar_acc_free[u & 1]);
       }
-      tc_fence_before();
-      arrive(&bar_acc_free[j & 1]);
+      if (!ok) break;
       asm volatile("bar.sync 1, %0;" ::"n"(kEpilogue) : "memory");
       float2* dst = s + base_ring[j % (2 * S)];
 #pragma unroll
@@ -562,25 +596,35 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   } else if (warp == 12 && lane == 0) {
     // ------------------------------------------------------------ MMA issue
-    constexpr uint32_t idesc = tf32_idesc<N>();
+    constexpr uint32_t idesc = tf32_idesc<Cfg::NH>();
     const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
-    for (uint64_t j = 0; j < count; ++j) {
-      if (!wait(&bar_a_ready[j & 1], (uint32_t)((j >> 1) & 1))) break;
-      if (j >= 2 && !wait(&bar_acc_free[j & 1], (uint32_t)(((j >> 1) - 1) & 1))) break;
-      tc_fence_after();
-      const uint32_t acc = tmem + (uint32_t)(2 * Cfg::A_COLS + (j & 1) * Cfg::ACC_COLS);
-      const uint32_t ah = tmem + (uint32_t)((j & 1) * Cfg::A_COLS);
+    bool ok = true;
+    for (uint64_t j = 0; j < count && ok; ++j) {
+      if (!wait(&bar_a_ready[j % Cfg::A_BUFS], (uint32_t)((j / Cfg::A_BUFS) & 1))) break;
+      const uint32_t ah = tmem + (uint32_t)((j % Cfg::A_BUFS) * Cfg::A_COLS);
       const uint32_t al = ah + (uint32_t)K;
+      for (int h = 0; h < Cfg::PASSES; ++h) {
+        const uint64_t u = j * Cfg::PASSES + h;
+        if (u >= 2 && !wait(&bar_acc_free[u & 1], (uint32_t)(((u >> 1) - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS);
+        // this pass's B rows (output columns) h*NH .. h*NH+NH-1: whole 8-row
+        // groups of each 128-byte K atom, so only the start address moves
+        const uint32_t hoff = (uint32_t)(h * Cfg::NH * 128);
 #pragma unroll
-      for (int st = 0; st < Cfg::KSTEPS; ++st) {
-        const uint32_t kbo = (uint32_t)((st >> 2) * N * 128 + (st & 3) * 32);
-        // main term hi*hi in its own accumulator; the two correction terms
-        // (2^-11 smaller) in a second one, summed in FP32 by the epilogue
-        tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
-        tc_mma_tf32_ts(acc + N, ah + 8 * st, sw128_desc(bl + kbo), idesc, st > 0 ? 1u : 0u);
-        tc_mma_tf32_ts(acc + N, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
+        for (int st = 0; st < Cfg::KSTEPS; ++st) {
+          const uint32_t kbo = (uint32_t)((st >> 2) * N * 128 + (st & 3) * 32) + hoff;
+          // main term hi*hi in its own accumulator; the two correction terms
+          // (2^-11 smaller) in a second one, summed in FP32 by the epilogue
+          tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
+          tc_mma_tf32_ts(acc + Cfg::NH, ah + 8 * st, sw128_desc(bl + kbo), idesc, st > 0 ? 1u : 0u);
+          tc_mma_tf32_ts(acc + Cfg::NH, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
+        }
+        tc_commit(smem_u32(&bar_mma[u & 1]));
       }
-      tc_commit(smem_u32(&bar_mma[j & 1]));
     }
   }
   tc_fence_before();
@@ -776,7 +820,7 @@ uint32_t host_tf32_rna(float x) {
 
 }  // namespace
 
-bool tc_supported(int k) { return k == 4 || k == 5; }
+bool tc_supported(int k) { return k >= 4 && k <= 6; }
 
 size_t tc_image_bytes(int k) {
   const size_t dim = size_t{1} << k;
@@ -814,13 +858,15 @@ void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& 
 void launch_fused_tc(const State& s, const Pass& p, const void* b_image) {
   if (p.k == 5) launch_tc<5>(s, p, b_image);
   else if (p.k == 4) launch_tc<4>(s, p, b_image);
-  else fail(KETGPU_ERR_LOGIC, "tensor-core block supports k = 4 or 5");
+  else if (p.k == 6) launch_tc<6>(s, p, b_image);
+  else fail(KETGPU_ERR_LOGIC, "tensor-core block supports k = 4, 5 or 6");
 }
 
 void tc_form(int n, const Pass& p, int* tma_dims, int* direct) {
-  if (p.k != 4 && p.k != 5) fail(KETGPU_ERR_LOGIC, "tensor-core block supports k = 4 or 5");
+  if (p.k < 4 || p.k > 6) fail(KETGPU_ERR_LOGIC, "tensor-core block supports k = 4, 5 or 6");
   TcGeom g;
   if (p.k == 5) tile_geometry<5>(n, p, g);
+  else if (p.k == 6) tile_geometry<6>(n, p, g);
   else tile_geometry<4>(n, p, g);
   int start[16], tq[16];
   const int nd = p.qubits[0] >= tc_tma_min() ? tile_runs(g, p.k + kGroupBits, start, tq) : 0;

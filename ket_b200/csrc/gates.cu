@@ -448,11 +448,138 @@ void launch_fused_simt(const State& st, const Pass& p, const void* mat_t) {
   KB_CUDA(cudaGetLastError());
 }
 
+
+// ---------------------------------------------------------------------------
+// Shared-memory runs (the plain method's staging of low-qubit gates).  A run
+// of consecutive gates whose qubits all lie below kRunBits touches only
+// amplitudes inside aligned chunks of 2^kRunBits; a CTA loads a chunk with
+// coalesced 16-byte loads, applies each gate in turn in shared memory
+// (exactly the pair / phase updates of the per-gate kernels, on chunk-local
+// indices), and stores the chunk back: one HBM pass for the run instead of
+// one per gate.
+
+template <typename R>
+struct RunGate {
+  int32_t kind;  // 0 pair (mode below), 1 phase
+  int32_t mode;  // kPairGeneral / kPairSwap / kPairDiag
+  int32_t nfixed;
+  int32_t fixed[3];
+  uint32_t p0, p1;
+  R re[4], im[4];
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+    run_kernel(typename C2<R>::T* __restrict__ s, uint64_t n_chunks, int bits,
+               const RunGate<R>* __restrict__ gates, int ngates) {
+  using T = typename C2<R>::T;
+  extern __shared__ __align__(16) unsigned char run_smem[];
+  T* sm = reinterpret_cast<T*>(run_smem);
+  RunGate<R>* sg = reinterpret_cast<RunGate<R>*>(run_smem + (sizeof(T) << kRunBits));
+  for (int i = threadIdx.x; i < ngates; i += kThreads) sg[i] = gates[i];
+  const int size = 1 << bits;
+  constexpr int V = 16 / (int)sizeof(T);  // amplitudes per 16-byte word
+  for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+    T* src = s + (c << bits);
+    __syncthreads();
+    for (int i = threadIdx.x; i < size / V; i += kThreads)
+      reinterpret_cast<float4*>(sm)[i] = reinterpret_cast<const float4*>(src)[i];
+    __syncthreads();
+    for (int gi = 0; gi < ngates; ++gi) {
+      const RunGate<R>& g = sg[gi];
+      const int cnt = size >> g.nfixed;
+      for (int i = threadIdx.x; i < cnt; i += kThreads) {
+        const uint32_t base = (uint32_t)spread((uint64_t)i, g.fixed, g.nfixed);
+        if (g.kind == 1) {
+          const T a = sm[base | g.p0];
+          T x;
+          x.x = g.re[0] * a.x - g.im[0] * a.y;
+          x.y = g.re[0] * a.y + g.im[0] * a.x;
+          sm[base | g.p0] = x;
+          continue;
+        }
+        const T a = sm[base | g.p0], b = sm[base | g.p1];
+        T x, y;
+        if (g.mode == kPairSwap) {
+          x = b;
+          y = a;
+        } else if (g.mode == kPairDiag) {
+          x.x = g.re[0] * a.x - g.im[0] * a.y;
+          x.y = g.re[0] * a.y + g.im[0] * a.x;
+          y.x = g.re[3] * b.x - g.im[3] * b.y;
+          y.y = g.re[3] * b.y + g.im[3] * b.x;
+        } else {
+          x.x = g.re[0] * a.x - g.im[0] * a.y + g.re[1] * b.x - g.im[1] * b.y;
+          x.y = g.re[0] * a.y + g.im[0] * a.x + g.re[1] * b.y + g.im[1] * b.x;
+          y.x = g.re[2] * a.x - g.im[2] * a.y + g.re[3] * b.x - g.im[3] * b.y;
+          y.y = g.re[2] * a.y + g.im[2] * a.x + g.re[3] * b.y + g.im[3] * b.x;
+        }
+        sm[base | g.p0] = x;
+        sm[base | g.p1] = y;
+      }
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i < size / V; i += kThreads)
+      reinterpret_cast<float4*>(src)[i] = reinterpret_cast<const float4*>(sm)[i];
+  }
+}
+
+template <typename R>
+void append_run_gates(const std::vector<Pass>& gates, std::vector<unsigned char>& out) {
+  for (const Pass& p : gates) {
+    RunGate<R> g{};
+    g.kind = p.kind == PassKind::Phase ? 1 : 0;
+    g.mode = p.mode;
+    g.nfixed = p.nfixed;
+    for (int j = 0; j < 3; ++j) g.fixed[j] = p.fixed[j];
+    g.p0 = (uint32_t)p.p0;
+    g.p1 = (uint32_t)p.p1;
+    for (int j = 0; j < 4; ++j) {
+      g.re[j] = (R)p.m[j].real();
+      g.im[j] = (R)p.m[j].imag();
+    }
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&g);
+    out.insert(out.end(), b, b + sizeof g);
+  }
+}
+
 }  // namespace
+
+void run_device_data(const std::vector<Pass>& gates, int precision, std::vector<unsigned char>& out) {
+  out.clear();
+  if (precision == KETGPU_C64) append_run_gates<float>(gates, out);
+  else append_run_gates<double>(gates, out);
+}
+
+void launch_run(const State& st, const Pass& p, const void* data) {
+  const int bits = st.n < kRunBits ? st.n : kRunBits;
+  const uint64_t n_chunks = st.dim() >> bits;
+  static int sms[64] = {0};
+  if (!sms[st.device]) sms[st.device] = sm_count(st.device);
+  uint64_t grid = (uint64_t)sms[st.device] * 8;
+  if (grid > n_chunks) grid = n_chunks;
+  if (st.precision == KETGPU_C64) {
+    const size_t smem = (sizeof(float2) << kRunBits) + sizeof(RunGate<float>) * (size_t)p.n_gates;
+    run_kernel<float><<<(unsigned)grid, kThreads, smem, st.stream>>>(
+        static_cast<float2*>(st.amps), n_chunks, bits, static_cast<const RunGate<float>*>(data), p.n_gates);
+  } else {
+    const size_t smem = (sizeof(double2) << kRunBits) + sizeof(RunGate<double>) * (size_t)p.n_gates;
+    static bool attr[64] = {false};
+    if (!attr[st.device]) {
+      KB_CUDA(cudaFuncSetAttribute(run_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)((sizeof(double2) << kRunBits) + sizeof(RunGate<double>) * kRunMaxGates)));
+      attr[st.device] = true;
+    }
+    run_kernel<double><<<(unsigned)grid, kThreads, smem, st.stream>>>(
+        static_cast<double2*>(st.amps), n_chunks, bits, static_cast<const RunGate<double>*>(data), p.n_gates);
+  }
+  count_launch();
+  KB_CUDA(cudaGetLastError());
+}
 
 double Pass::bytes(int n, size_t amp) const {
   const double dim = (double)(uint64_t{1} << n);
-  if (kind == PassKind::Fused || kind == PassKind::Diagonal) return 2.0 * amp * dim;
+  if (kind == PassKind::Fused || kind == PassKind::Diagonal || kind == PassKind::SharedRun) return 2.0 * amp * dim;
   if (kind == PassKind::NormCapture) return amp * dim;
   if (kind == PassKind::NormRestore) return 3.0 * amp * dim;
   if (kind == PassKind::Phase) return 2.0 * amp * dim / (double)(uint64_t{1} << nfixed);
@@ -484,6 +611,10 @@ void launch_pass(const State& s, const Plan& plan, const Pass& p) {
   }
   if (p.kind == PassKind::Diagonal) {
     launch_diag(s, p, static_cast<const char*>(plan.d_diag) + plan.offdiag[p.diag_index]);
+    return;
+  }
+  if (p.kind == PassKind::SharedRun) {
+    launch_run(s, p, static_cast<const char*>(plan.d_runs) + plan.offrun[p.run_index]);
     return;
   }
   if (p.kind != PassKind::Fused) {

@@ -68,7 +68,13 @@ enum class PassKind : int {
   NormRestore,  // rescale the state to the recorded squared norm
   Diagonal,     // multiply amplitude x by exp(i phi(x)), phi a quadratic
                 // polynomial in the index bits (a run of diagonal gates)
+  SharedRun,    // consecutive gates on qubits below kRunBits, applied one
+                // after another to chunks of 2^kRunBits amplitudes held in
+                // shared memory (one HBM pass for the run)
 };
+// Chunk bits of a shared-memory run: its gates act on qubits 0..kRunBits-1.
+constexpr int kRunBits = 11;
+constexpr int kRunMaxGates = 128;
 enum PairMode : int { kPairGeneral = 0, kPairSwap = 1, kPairDiag = 2 };
 
 struct Pass {
@@ -84,6 +90,7 @@ struct Pass {
   size_t mat_index = 0;                // into Plan::matrices
   bool tensor = false;                 // tcgen05 path
   size_t diag_index = 0;               // Diagonal: into Plan::diags
+  size_t run_index = 0;                // SharedRun: into Plan::runs
   int first_op = 0, n_gates = 0;       // provenance
   std::vector<int> gates;              // op indices of the gates this pass applies
   double bytes(int n, size_t amp) const;
@@ -114,7 +121,9 @@ struct Plan {
   double* d_norm = nullptr;  // [captured, current, block partials...]
   std::vector<DiagPoly> diags;  // Diagonal passes (host)
   void* d_diag = nullptr;       // per Diagonal pass: low-bit table + coefficients
-  std::vector<size_t> off64, off32, offtc, offdiag;
+  std::vector<std::vector<Pass>> runs;  // SharedRun passes: each gate lowered (host)
+  void* d_runs = nullptr;               // their device gate records
+  std::vector<size_t> off64, off32, offtc, offdiag, offrun;
   int device = -1;
   ketgpu_plan_stats stats{};
   ~Plan();
@@ -169,6 +178,9 @@ void tc_form(int n, const Pass& p, int* tma_dims, int* direct);
 // Diagonal pass: device data = table (2^L complex, state precision) then FP64
 // coefficients, laid out by diag_device_data (diag.cu).
 void launch_diag(const State& s, const Pass& p, const void* data);
+// SharedRun pass: device gate records laid out by run_device_data (gates.cu).
+void launch_run(const State& s, const Pass& p, const void* data);
+void run_device_data(const std::vector<Pass>& gates, int precision, std::vector<unsigned char>& out);
 void diag_device_data(const DiagPoly& poly, int n, int precision, std::vector<unsigned char>& out);
 bool is_diagonal_gate(int type);
 // Add one diagonal gate's phase terms to a polynomial.

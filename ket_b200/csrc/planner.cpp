@@ -252,7 +252,7 @@ uint64_t qubit_mask(const ketgpu_op& o) {
 // plus the compute that outgrows it at large k.
 double fused_cost_static(int k, int precision, bool tensor) {
   if (precision == KETGPU_C128) return k <= 4 ? 1.0 : (k == 5 ? 1.35 : 2.7);
-  if (tensor && (k == 4 || k == 5)) return 1.0;
+  if (tensor && k >= 4 && k <= 6) return 1.0;
   return k <= 4 ? 1.0 : (k == 5 ? 1.45 : 2.9);
 }
 
@@ -383,6 +383,19 @@ void emit_single(Plan& plan, const ketgpu_op& o, int idx) {
   p.first_op = idx;
   p.n_gates = 1;
   p.gates = {idx};
+  plan.passes.push_back(p);
+}
+
+void emit_run(Plan& plan, const ketgpu_op* ops, const std::vector<int>& gates) {
+  std::vector<Pass> lowered;
+  for (int gi : gates) lowered.push_back(lower_gate(ops[gi]));
+  Pass p;
+  p.kind = PassKind::SharedRun;
+  p.run_index = plan.runs.size();
+  p.first_op = gates.front();
+  p.n_gates = (int)gates.size();
+  p.gates = gates;
+  plan.runs.push_back(std::move(lowered));
   plan.passes.push_back(p);
 }
 
@@ -522,7 +535,21 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
   auto flush = [&]() {
     if (seg.empty()) return;
     if (opt.fusion == KETGPU_FUSE_NONE) {
-      for (int idx : seg) emit_single(plan, ops[idx], idx);
+      // One kernel per gate, except that consecutive gates on qubits below
+      // kRunBits are staged through shared memory as one pass.
+      const int bits = std::min(n, kRunBits);
+      size_t i = 0;
+      while (i < seg.size()) {
+        size_t j = i;
+        while (j < seg.size() && j - i < (size_t)kRunMaxGates && (qubit_mask(ops[seg[j]]) >> bits) == 0) ++j;
+        if (j - i >= 2) {
+          emit_run(plan, ops, std::vector<int>(seg.begin() + i, seg.begin() + j));
+          i = j;
+        } else {
+          emit_single(plan, ops[seg[i]], seg[i]);
+          ++i;
+        }
+      }
     } else if (opt.fusion == KETGPU_FUSE_REFERENCE) {
       for (const Block& b : reference_blocks(ops, seg)) {
         if (b.gates.size() == 1) emit_single(plan, ops[b.gates[0]], b.gates[0]);

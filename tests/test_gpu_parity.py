@@ -91,6 +91,10 @@ TARGETS = {
     "low5": [0, 1, 2, 3, 4], "high5": None, "mixed5": [0, 3, 7, 11, 13], "spread5": [1, 5, 8, 12, 15],
     "q1tgt5": [1, 6, 9, 12, 14], "q2tgt5": [2, 7, 9, 11, 13],
     "low4": [0, 1, 2, 3], "mixed4": [2, 6, 9, 14], "high4": None, "q3tgt4": [3, 7, 10, 14],
+    # k = 6: two MMA passes of half the output columns per tile, one A region
+    "low6": [0, 1, 2, 3, 4, 5], "high6": None, "mixed6": [0, 3, 7, 11, 13, 15],
+    "spread6": [1, 5, 8, 12, 15, 17], "q1tgt6": [1, 6, 9, 12, 14, 15], "q2tgt6": [2, 7, 9, 11, 13, 15],
+    "q2run6": [2, 3, 4, 5, 6, 7], "q6run6": [6, 7, 8, 9, 10, 11],
 }
 
 
@@ -99,11 +103,11 @@ TARGETS = {
 def test_tensor_core_block_positions(oracle, name, n):
     """Single dense blocks on the tcgen05 path at every kind of target set."""
     import ket_b200 as kb
-    k = 5 if name.endswith("5") else 4
+    k = int(name[-1])
     qs = TARGETS[name] or list(range(n - k, n))
     qs = [q for q in qs if q < n]
-    if len(qs) != k:
-        pytest.skip("targets outside the register")
+    if len(qs) != k or n < k + 7:
+        pytest.skip("targets outside the register, or too few qubits for a 128-group tile")
     prep = _block_circuit(n, list(range(n)), seed=n, depth=2 * n)  # generic input state
     blk = _block_circuit(n, qs, seed=100 + n)
     ops = np.concatenate([prep, blk])
