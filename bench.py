@@ -487,6 +487,15 @@ def main():
         "per_gate_ms": float(per_pass[other].sum()) if other else 0.0,
         "hbm_gbs_all_passes": float(stats["bytes"] / (per_pass.sum() * 1e-3) / 1e9),
     }
+    # dense blocks by producer / epilogue form (tensor copy or cp.async,
+    # direct or staged stores): count and mean GB/s of algorithmic bytes
+    forms = {}
+    for i in tc_idx:
+        f = plan.pass_tc_form(i)
+        key = ("tensor_copy" if f["tma_dims"] else "cp_async") + ("_direct" if f["direct"] else "_staged")
+        forms.setdefault(key, []).append(info[i][3] / (per_pass[i] * 1e-3) / 1e9)
+    pass_summary["dense_tc_by_form"] = {k: {"blocks": len(v), "mean_gbs": float(np.mean(v))}
+                                        for k, v in sorted(forms.items())}
 
     # e2e through the C ABI with host buffers
     e2e = None

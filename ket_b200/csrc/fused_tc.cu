@@ -649,10 +649,12 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// Lowest target qubit from which a block uses the tensor-copy producer
-// (default 2: qubits 0 and 1 group bits).  KETGPU_TC_TMA=0 keeps every block
-// on the cp.async producers, KETGPU_TC_TMA_MIN=q raises the threshold (for
-// comparing the producer forms on one workload).
+// Lowest target qubit from which a block always uses the tensor-copy
+// producer (default 2: qubits 0 and 1 group bits).  A block whose lowest
+// target is qubit 1 uses it when its converter reads stay conflict-free
+// (tma_read_wavefronts).  KETGPU_TC_TMA=0 keeps every block on the cp.async
+// producers, KETGPU_TC_TMA_MIN=q raises the threshold (for comparing the
+// producer forms on one workload).
 int tc_tma_min() {
   static const int v = [] {
     const char* e = std::getenv("KETGPU_TC_TMA");
@@ -724,6 +726,58 @@ int sm_count_tc(int device) {
   return v;
 }
 
+// Shared-memory wavefronts of the worst converter read of a tensor-copy tile
+// (host only): lane l of converter warp q reads, for each combination c, the
+// 8-byte amplitude of group 32q + l at its natural tile offset under the
+// 128-byte swizzle.  A warp's 32 reads need at least 2 wavefronts; more
+// means lanes whose groups lie 1 KB or more apart share banks.
+int tma_read_wavefronts(const TcGeom& g, int tb, int dim) {
+  int worst = 0;
+  for (int q = 0; q < 4; ++q)
+    for (int c = 0; c < dim; ++c) {
+      uint32_t ctile = 0;
+      for (int b = 0, jb = 0; jb < tb; ++jb)
+        if (g.is_target[jb]) {
+          if ((c >> b) & 1) ctile |= 8u << jb;
+          ++b;
+        }
+      uint32_t words[32][2];
+      for (int l = 0; l < 32; ++l) {
+        const int lane_row = 32 * q + l;
+        uint32_t gtile = 0;
+        for (int jb = 0, gb = 0; jb < tb; ++jb)
+          if (!g.is_target[jb]) {
+            if ((lane_row >> gb) & 1) gtile |= 8u << jb;
+            ++gb;
+          }
+        const uint32_t off = ctile | gtile;
+        const uint32_t addr = off ^ ((off >> 3) & 0x70u);
+        words[l][0] = addr >> 2;
+        words[l][1] = (addr >> 2) + 1;
+      }
+      for (int bank = 0; bank < 32; ++bank) {
+        uint32_t seen[64];
+        int ns = 0;
+        for (int l = 0; l < 32; ++l)
+          for (int w = 0; w < 2; ++w)
+            if ((words[l][w] & 31u) == (uint32_t)bank) {
+              bool dup = false;
+              for (int i = 0; i < ns; ++i) dup |= seen[i] == words[l][w];
+              if (!dup) seen[ns++] = words[l][w];
+            }
+        worst = ns > worst ? ns : worst;
+      }
+    }
+  return worst;
+}
+
+// Whether a block takes the tensor-copy producer (before the tile-run limits).
+bool tma_wanted(const TcGeom& g, const Pass& p, int tb) {
+  const int lowest = p.qubits[0];
+  if (lowest >= tc_tma_min()) return true;
+  return lowest == 1 && tc_tma_min() <= 2 && tma_read_wavefronts(g, tb, 1 << p.k) <= 2;
+}
+
 // Tile layout of a block on an n-qubit state (host only): the tile qubits,
 // the tile index decomposition, each combination's offset and the
 // cp.async-form direct-store rule.
@@ -780,8 +834,8 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   tile_geometry<KQ>(st.n, p, g);
   CUtensorMap tmap;
   std::memset(&tmap, 0, sizeof(tmap));
-  // Tensor-copy blocks (qubits 0 and 1 group bits) always store directly.
-  g.tma_dims = p.qubits[0] >= tc_tma_min() ? encode_tile_map(st, g, Cfg::TB, &tmap) : 0;
+  // Tensor-copy blocks (qubit 0 a group bit) always store directly.
+  g.tma_dims = tma_wanted(g, p, Cfg::TB) ? encode_tile_map(st, g, Cfg::TB, &tmap) : 0;
   if (g.tma_dims) {
     g.direct = 1;
     for (int c = 0; c < Cfg::DIM; ++c) {
@@ -869,7 +923,7 @@ void tc_form(int n, const Pass& p, int* tma_dims, int* direct) {
   else if (p.k == 6) tile_geometry<6>(n, p, g);
   else tile_geometry<4>(n, p, g);
   int start[16], tq[16];
-  const int nd = p.qubits[0] >= tc_tma_min() ? tile_runs(g, p.k + kGroupBits, start, tq) : 0;
+  const int nd = tma_wanted(g, p, p.k + kGroupBits) ? tile_runs(g, p.k + kGroupBits, start, tq) : 0;
   *tma_dims = nd;
   *direct = nd ? 1 : g.direct;
 }
