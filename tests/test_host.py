@@ -131,8 +131,11 @@ def test_tensor_core_producer_forms():
     """Which tensor-core blocks fetch tiles with one tensor copy (and how many
     tensor-map dimensions), and which store straight from registers: the
     first tensor-copy dimension is qubits 0-3, later ones hold runs of at
-    most 8 tile qubits, at most 5 in all; blocks targeting qubit 0 or 1 keep
-    the cp.async producers."""
+    most 8 tile qubits, at most 5 in all; blocks targeting qubit 0 keep the
+    cp.async producers, and blocks whose lowest target is qubit 1 take the
+    tensor copy only when their converter reads stay conflict-free (1 3 5 7 9
+    and 1 2 25 26 27 do, measured 4.6 -> 5.8-5.9 TB/s; 1 2 3 4 5 does not,
+    measured 4.9 -> 4.4 TB/s)."""
     import collections
     import ket_b200 as ket
     from ket_b200.api import Plan
@@ -146,11 +149,11 @@ def test_tensor_core_producer_forms():
             f = p.pass_tc_form(i)
             forms[(f["tma_dims"], f["direct"])] += 1
             if f["tma_dims"]:
-                assert p.pass_qubits(i)[0] >= 2 and f["direct"]
+                assert p.pass_qubits(i)[0] >= 1 and f["direct"]
         else:
             with pytest.raises(ValueError):
                 p.pass_tc_form(i)
-    assert forms == {(2, True): 20, (3, True): 66, (4, True): 40, (0, False): 18}
+    assert forms == {(2, True): 20, (3, True): 69, (4, True): 40, (0, False): 15}
     # 4-qubit blocks (11-qubit tiles): the same rule
     p4 = Plan(30, random_brickwork(30, 40).to_ops(), ket.make_options("c64", "greedy", 4, True))
     for i in range(p4.stats()["n_passes"]):
@@ -159,12 +162,14 @@ def test_tensor_core_producer_forms():
             assert info["k"] == 4
             f = p4.pass_tc_form(i)
             assert 0 <= f["tma_dims"] <= 5
-            assert (f["tma_dims"] > 0) == (p4.pass_qubits(i)[0] >= 2)
+            low = p4.pass_qubits(i)[0]
+            assert (f["tma_dims"] > 0) == (low >= 2) or low == 1
             assert f["direct"] or f["tma_dims"] == 0
 
     expect = {(10, 11, 12, 13, 14): (3, True), (5, 6, 23, 24, 25): (3, True), (8, 9, 10, 13, 14): (4, True),
               (2, 3, 4, 5, 6): (2, True), (3, 4, 5, 14, 15): (3, True), (8, 10, 12, 14, 16): (0, True),
-              (3, 9, 14, 20, 27): (0, True), (1, 3, 5, 7, 9): (0, False), (0, 1, 2, 3, 4): (0, False)}
+              (3, 9, 14, 20, 27): (0, True), (1, 3, 5, 7, 9): (2, True), (1, 2, 25, 26, 27): (3, True),
+              (1, 2, 3, 4, 5): (0, False), (0, 1, 2, 3, 4): (0, False)}
     for qs, want in expect.items():
         c = ket.Circuit(28)
         for q in qs:
