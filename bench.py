@@ -355,6 +355,66 @@ def run_adjoint24(args):
     print(json.dumps(line), flush=True)
 
 
+def run_kernels26(args):
+    """Every kernel family once on a 26-qubit state (1 GiB complex128 /
+    512 MiB complex64, larger than L2): per-gate pair / phase kernels and
+    shared-memory runs (plain method, both precisions), FP64 dense blocks,
+    tensor-core blocks at k = 4, 5, 6, a diagonal run, batched Pauli terms,
+    the sampling tree and descent, and the cost model's forward, backward
+    and Adam kernels.  Prints each pass kind's time and algorithmic GB/s
+    (CUDA events, ketgpu_plan_execute_timed); the profile summaries under
+    profiles/ come from ncu runs of this workload."""
+    import ket_b200 as ket
+    from ket_b200.planner import CostModel
+    from ket_b200.workloads import qft_ghz_rz, random_mixed, random_pauli_sum
+    n = args.qubits if args.qubits != N_QUBITS else 26
+    kinds = {0: "pair", 1: "phase", 2: "dense_block", 3: "norm", 4: "diagonal_run", 5: "shared_run"}
+    out = {"metric": "per-kernel time and algorithmic GB/s, 26 qubits", "qubits": n, "passes": {}}
+    circ = random_mixed(n, 6, seed=5)
+    ops = circ.to_ops()
+    cases = [("c64", "none", 5, True), ("c128", "none", 5, True), ("c128", "greedy", 5, True),
+             ("c64", "greedy", 4, True), ("c64", "greedy", 5, True), ("c64", "greedy", 6, True)]
+    for prec, fusion, k, tc in cases:
+        plan = ket.Plan(n, ops, ket.make_options(prec, fusion, k, tc))
+        st = ket.DeviceState(n, prec)
+        ms = np.zeros(int(plan.stats()["n_passes"]), dtype=np.float32)
+        from ket_b200 import _lib
+        for _ in range(max(1, args.warmup)):
+            st.reset()
+            _lib.check(_lib.lib.ketgpu_plan_execute_timed(plan._h, st.handle, ms.ctypes.data))
+        agg = {}
+        for i in range(len(ms)):
+            info = plan.pass_info(i)
+            key = f"{prec}/{fusion}/k{k}/{kinds[info['kind']]}" + (f"/k{info['k']}" if info["kind"] == 2 else "")
+            a = agg.setdefault(key, [0, 0.0, 0.0])
+            a[0] += 1
+            a[1] += float(ms[i])
+            a[2] += info["bytes"]
+        for key, (cnt, t, b) in agg.items():
+            out["passes"][key] = {"launches": cnt, "ms": t, "gbs": b / (t * 1e-3) / 1e9 if t > 0 else None}
+        st.close()
+        plan.close()
+    # diagonal run (QFT pattern) and reductions on one complex64 state
+    d = ket.run_device(qft_ghz_rz(n, seed=7), options=ket.make_options("c64", "greedy", 5, True))
+    ham = random_pauli_sum(n, 64, seed=11)
+    t0 = time.perf_counter()
+    d.expval(ham)
+    out["expval_64_terms_ms_e2e"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    d.sample_seeded(42, 10 ** 6)
+    out["sample_1e6_ms_e2e"] = (time.perf_counter() - t0) * 1e3
+    d.close()
+    # cost model: forward on 4096 rows, one gradient evaluation, 200 Adam steps
+    m = CostModel(seed=3)
+    x = np.random.default_rng(1).standard_normal((4096, 48)).astype(np.float32)
+    y = np.random.default_rng(2).standard_normal(4096).astype(np.float32)
+    m.forward(x)
+    m.gradients(x, y)
+    m.train(x, y, steps=200, minibatch=512)
+    m.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,7 +430,7 @@ def main():
     ap.add_argument("--k", type=int, default=5)
     ap.add_argument("--qubits", type=int, default=N_QUBITS, help="smaller cases for profiling only")
     ap.add_argument("--depth", type=int, default=DEPTH)
-    ap.add_argument("--workload", default="circuit30", choices=["circuit30", "sample33", "adjoint24"])
+    ap.add_argument("--workload", default="circuit30", choices=["circuit30", "sample33", "adjoint24", "kernels26"])
     ap.add_argument("--shots", type=int, default=1000000)
     ap.add_argument("--batch", type=int, default=64)
     args = ap.parse_args()
@@ -380,6 +440,8 @@ def main():
         return run_sample33(args)
     if args.workload == "adjoint24":
         return run_adjoint24(args)
+    if args.workload == "kernels26":
+        return run_kernels26(args)
 
     rank, world, local = init_dist(args.gpus)
     import ket_b200 as ket

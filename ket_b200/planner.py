@@ -193,7 +193,8 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=1500)
     ap.add_argument("--eval", type=int, default=500)
-    ap.add_argument("--train-gates", type=int, default=48, help="gates of each training circuit that are timed")
+    ap.add_argument("--train-gates", type=int, default=0,
+                    help="gates of each training circuit that are timed (0: the whole circuit)")
     ap.add_argument("--check", type=int, default=60, help="held-out circuits whose states are compared")
     ap.add_argument("--unfused", type=int, default=60, help="held-out circuits also timed unfused")
     ap.add_argument("--steps", type=int, default=4000)
@@ -214,8 +215,10 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
         train_spec = []
     for j, (n, d, s) in enumerate(train_spec):
         c = random_mixed(n, d, seed=s)
-        sub = Circuit(n)
-        sub._gates = c.gates[:args.train_gates]
+        sub = c
+        if args.train_gates > 0:
+            sub = Circuit(n)
+            sub._gates = c.gates[:args.train_gates]
         x, y = measure_passes(sub)
         X.append(x)
         Y.append(y)
@@ -223,6 +226,7 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
             print(f"measured {j}/{len(train_spec)} circuits, {sum(len(a) for a in X)} rows, "
                   f"{time.time() - t0:.0f} s", flush=True)
     t_measure = time.time() - t0
+    curve = []
     if args.load:
         model = CostModel.load(args.load)
         X = np.zeros((0, NF), dtype=np.float32)
@@ -236,8 +240,14 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
         model = CostModel(seed=7)
         loss0 = float(np.mean((model.forward(X) - Y) ** 2))
         t1 = time.time()
-        loss = model.train(X, Y, steps=args.steps, minibatch=512, lr=2e-3)
-        loss = model.train(X, Y, steps=args.steps // 2, minibatch=512, lr=5e-4)
+        # Adam in the library's kernels, in 30 legs; the full-batch mean
+        # squared error after each leg is the loss curve
+        curve = []
+        legs = [(args.steps // 20, 2e-3)] * 20 + [(args.steps // 20, 5e-4)] * 10
+        for steps, lr in legs:
+            model.train(X, Y, steps=max(1, steps), minibatch=512, lr=lr)
+            curve.append(float(np.mean((model.forward(X) - Y) ** 2)))
+        loss = curve[-1]
         t_train = time.time() - t1
         pred = model.forward(X)
         train_rmse = float(np.sqrt(np.mean((pred - Y) ** 2)))
@@ -303,11 +313,15 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     un = [(r["unfused_ms"], r["greedy_ms"], r["learned_ms"]) for r in rows if "unfused_ms" in r]
     errs = [max(r["greedy_max_abs_vs_unfused"], r["learned_max_abs_vs_unfused"]) for r in rows
             if "greedy_max_abs_vs_unfused" in r]
+    import hashlib
+    model_path = args.load or args.save
     summary = {
-        "model": args.load or args.save,
-        "train_circuits": len(train_spec), "eval_circuits": len(eval_spec), "train_rows": int(len(X)),
+        "model": model_path,
+        "model_sha256": hashlib.sha256(open(model_path, "rb").read()).hexdigest(),
+        "train_circuits": len(train_spec), "train_gates_per_circuit": args.train_gates or "all",
+        "eval_circuits": len(eval_spec), "train_rows": int(len(X)),
         "measure_s": t_measure, "train_s": t_train, "loss_initial": loss0, "loss_final": loss,
-        "train_rmse_log_us": train_rmse,
+        "loss_curve": curve, "train_rmse_log_us": train_rmse,
         "eval_total_greedy_ms": float(gt.sum()), "eval_total_learned_ms": float(lt.sum()),
         "eval_learned_over_greedy": float(lt.sum() / gt.sum()),
         "eval_learned_over_greedy_geomean": float(np.exp(np.mean(np.log(lt / gt)))),
