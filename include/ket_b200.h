@@ -150,6 +150,14 @@ int ketgpu_plan_pass_info(const ketgpu_plan* p, uint64_t index, int32_t* kind, i
  * passes and diagonal runs, which touch every qubit). */
 int ketgpu_plan_pass_qubits(const ketgpu_plan* p, uint64_t index, int32_t* qubits,
                             int32_t capacity, int32_t* count);
+/* The circuit ops (indices into the plan's op array) that pass `index`
+ * applies, in the order it applies them.  The planner may reorder commuting
+ * gates (its band orders), so the passes' gate lists, concatenated, are a
+ * topological order of the circuit's gates.  Writes min(count, capacity)
+ * entries; *count receives the full number (0 for norm passes).  Host only;
+ * no counterpart in ket. */
+int ketgpu_plan_pass_gates(const ketgpu_plan* p, uint64_t index, int32_t* gates,
+                           int32_t capacity, int32_t* count);
 /* How tensor-core pass `index` runs: tma_dims = dimensions of the tensor map
  * that fetches each tile with one tiled copy (0: per-thread cp.async), and
  * direct = 1 when the epilogue stores straight from registers (0: staged

@@ -78,6 +78,7 @@ def _load():
         "ketgpu_plan_execute_timed": ([vp, vp, vp], ct.c_int),
         "ketgpu_plan_pass_info": ([vp, u64, ct.POINTER(i32), ct.POINTER(i32), ct.POINTER(i32), pd], ct.c_int),
         "ketgpu_plan_pass_qubits": ([vp, u64, ct.POINTER(i32), i32, ct.POINTER(i32)], ct.c_int),
+        "ketgpu_plan_pass_gates": ([vp, u64, ct.POINTER(i32), i32, ct.POINTER(i32)], ct.c_int),
         "ketgpu_release_cache": ([], ct.c_int),
         "ketgpu_run_last_profile": ([vp], ct.c_int),
         "ketgpu_plan_pass_tc_form": ([vp, u64, ct.POINTER(i32), ct.POINTER(i32)], ct.c_int),

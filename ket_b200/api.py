@@ -495,6 +495,14 @@ class Plan:
         check(lib.ketgpu_plan_pass_qubits(self._h, index, buf, 8, ct.byref(cnt)))
         return [buf[i] for i in range(min(cnt.value, 8))]
 
+    def pass_gates(self, index: int) -> List[int]:
+        """Indices of the ops pass `index` applies, in its order."""
+        cnt = ct.c_int32()
+        check(lib.ketgpu_plan_pass_gates(self._h, index, None, 0, ct.byref(cnt)))
+        buf = (ct.c_int32 * max(1, cnt.value))()
+        check(lib.ketgpu_plan_pass_gates(self._h, index, buf, cnt.value, ct.byref(cnt)))
+        return list(buf[:cnt.value])
+
     def pass_tc_form(self, index: int) -> dict:
         """How a tensor-core pass runs: ``tma_dims`` (dimensions of the
         tensor map fetching each tile; 0 = per-thread cp.async) and

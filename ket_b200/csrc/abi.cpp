@@ -845,6 +845,19 @@ KB_API int ketgpu_plan_pass_qubits(const ketgpu_plan* p, uint64_t index, int32_t
   });
 }
 
+KB_API int ketgpu_plan_pass_gates(const ketgpu_plan* p, uint64_t index, int32_t* gates, int32_t capacity,
+                                  int32_t* count) {
+  return guard([&] {
+    need(p != nullptr && count != nullptr, "null argument");
+    need(capacity >= 0 && (capacity == 0 || gates != nullptr), "bad gate buffer");
+    const Plan& plan = *as_plan(p);
+    if (index >= plan.passes.size()) fail(KETGPU_ERR_OUT_OF_RANGE, "pass index out of range");
+    const Pass& ps = plan.passes[index];
+    for (size_t i = 0; i < ps.gates.size() && (int32_t)i < capacity; ++i) gates[i] = ps.gates[i];
+    *count = (int32_t)ps.gates.size();
+  });
+}
+
 KB_API int ketgpu_plan_pass_tc_form(const ketgpu_plan* p, uint64_t index, int32_t* tma_dims, int32_t* direct) {
   return guard([&] {
     need(p != nullptr && tma_dims != nullptr && direct != nullptr, "null argument");

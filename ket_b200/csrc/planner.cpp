@@ -353,6 +353,80 @@ std::vector<Block> grow_blocks(int n, const ketgpu_op* ops, const std::vector<in
   return blocks;
 }
 
+// Topological orders of a segment's gates for the greedy block growth.  The
+// program order is one; a "band" order of width w sorts the gates by
+// (ASAP depth / w, lowest qubit, depth), subject to every dependency, so
+// growth from the first gate follows a few neighbouring qubits through w
+// levels of the circuit before moving on: light-cone-shaped blocks.  On the
+// 30-qubit, 40-layer brick wall at k = 5 the best band order needs 119
+// passes against 154 in program order.  Returns op indices.
+std::vector<int> band_order(const ketgpu_op* ops, const std::vector<int>& seg, int n, int w) {
+  const size_t G = seg.size();
+  std::vector<int> depth(G, 0), indeg(G, 0), qmin(G, 0), last(n, -1);
+  std::vector<std::vector<int>> succ(G);
+  for (size_t i = 0; i < G; ++i) {
+    const ketgpu_op& o = ops[seg[i]];
+    int d = 0, lo = n;
+    for (int j = 0; j < gate_arity(o.type); ++j) {
+      const int q = o.q[j];
+      lo = std::min(lo, q);
+      if (last[q] >= 0) {
+        d = std::max(d, depth[last[q]] + 1);
+        succ[last[q]].push_back((int)i);
+        ++indeg[i];
+      }
+      last[q] = (int)i;
+    }
+    depth[i] = d;
+    qmin[i] = lo;
+  }
+  auto later = [&](int a, int b) {  // heap order: the smallest key first
+    const int ba = depth[a] / w, bb = depth[b] / w;
+    if (ba != bb) return ba > bb;
+    if (qmin[a] != qmin[b]) return qmin[a] > qmin[b];
+    if (depth[a] != depth[b]) return depth[a] > depth[b];
+    return a > b;
+  };
+  std::vector<int> heap, out;
+  out.reserve(G);
+  for (size_t i = 0; i < G; ++i)
+    if (!indeg[i]) heap.push_back((int)i);
+  std::make_heap(heap.begin(), heap.end(), later);
+  while (!heap.empty()) {
+    std::pop_heap(heap.begin(), heap.end(), later);
+    const int i = heap.back();
+    heap.pop_back();
+    out.push_back(seg[i]);
+    for (int sidx : succ[i])
+      if (--indeg[sidx] == 0) {
+        heap.push_back(sidx);
+        std::push_heap(heap.begin(), heap.end(), later);
+      }
+  }
+  return out;
+}
+
+// Band widths the planner tries besides the program order.
+constexpr int kBandWidths[] = {3, 4, 5, 6, 8};
+
+// Static cost of a partition in full-state passes: each block fused or as
+// its separate gates, whichever is cheaper; a diagonal run is one pass.
+double partition_cost(const ketgpu_op* ops, const std::vector<Block>& blocks, const PlanOptions& opt) {
+  double total = 0;
+  for (const Block& b : blocks) {
+    if (b.diag) {
+      total += 1.0;
+      continue;
+    }
+    double separate = 0;
+    for (int gi : b.gates) separate += gate_traffic_fraction(ops[gi]);
+    total += b.gates.size() > 1 ? std::min(separate, fused_cost_static((int)b.qubits.size(), opt.precision,
+                                                                         opt.tensor))
+                                : separate;
+  }
+  return total;
+}
+
 // ket's Fuser block rule on one barrier-free segment.
 std::vector<Block> reference_blocks(const ketgpu_op* ops, const std::vector<int>& order) {
   std::vector<Block> blocks;
@@ -660,7 +734,19 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
           for (int gi : b.gates) emit_single(plan, ops[gi], gi);
       }
     } else {
-      for (const Block& b : grow_blocks(n, ops, seg, std::max(1, opt.max_k), true)) {
+      // greedy growth over the program order and every band order; the
+      // partition with the least static cost wins (the program order on ties)
+      std::vector<Block> best = grow_blocks(n, ops, seg, std::max(1, opt.max_k), true);
+      double best_cost = partition_cost(ops, best, opt);
+      for (int w : kBandWidths) {
+        std::vector<Block> cand = grow_blocks(n, ops, band_order(ops, seg, n, w), std::max(1, opt.max_k), true);
+        const double c = partition_cost(ops, cand, opt);
+        if (c < best_cost - 1e-9) {
+          best = std::move(cand);
+          best_cost = c;
+        }
+      }
+      for (const Block& b : best) {
         if (b.diag) {
           emit_diagonal(plan, n, ops, b);
           continue;
