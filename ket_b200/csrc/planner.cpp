@@ -14,10 +14,12 @@
 //   * FUSE_LEARNED    the same candidate generator, with block costs from the
 //                     MLP cost model and the partition chosen by predicted time.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -355,12 +357,12 @@ std::vector<Block> grow_blocks(int n, const ketgpu_op* ops, const std::vector<in
 
 // Topological orders of a segment's gates for the greedy block growth.  The
 // program order is one; a "band" order of width w sorts the gates by
-// (ASAP depth / w, lowest qubit, depth), subject to every dependency, so
+// ((ASAP depth + offset) / w, lowest qubit, depth), subject to every dependency, so
 // growth from the first gate follows a few neighbouring qubits through w
 // levels of the circuit before moving on: light-cone-shaped blocks.  On the
 // 30-qubit, 40-layer brick wall at k = 5 the best band order needs 119
 // passes against 154 in program order.  Returns op indices.
-std::vector<int> band_order(const ketgpu_op* ops, const std::vector<int>& seg, int n, int w) {
+std::vector<int> band_order(const ketgpu_op* ops, const std::vector<int>& seg, int n, int w, int off) {
   const size_t G = seg.size();
   std::vector<int> depth(G, 0), indeg(G, 0), qmin(G, 0), last(n, -1);
   std::vector<std::vector<int>> succ(G);
@@ -381,7 +383,7 @@ std::vector<int> band_order(const ketgpu_op* ops, const std::vector<int>& seg, i
     qmin[i] = lo;
   }
   auto later = [&](int a, int b) {  // heap order: the smallest key first
-    const int ba = depth[a] / w, bb = depth[b] / w;
+    const int ba = (depth[a] + off) / w, bb = (depth[b] + off) / w;
     if (ba != bb) return ba > bb;
     if (qmin[a] != qmin[b]) return qmin[a] > qmin[b];
     if (depth[a] != depth[b]) return depth[a] > depth[b];
@@ -406,8 +408,9 @@ std::vector<int> band_order(const ketgpu_op* ops, const std::vector<int>& seg, i
   return out;
 }
 
-// Band widths the planner tries besides the program order.
-constexpr int kBandWidths[] = {3, 4, 5, 6, 8};
+// Band widths the planner tries besides the program order, each at every
+// offset (the band boundaries shifted by 0 .. w-1 levels).
+constexpr int kBandWidths[] = {3, 4, 5, 6, 7, 8};
 
 // Static cost of a partition in full-state passes: each block fused or as
 // its separate gates, whichever is cheaper; a diagonal run is one pass.
@@ -425,6 +428,40 @@ double partition_cost(const ketgpu_op* ops, const std::vector<Block>& blocks, co
                                 : separate;
   }
   return total;
+}
+
+// Greedy growth over the program order and every band order (width,
+// offset); the partition with the least static cost, the earliest candidate
+// on ties.  The candidates are grown on up to 16 host threads.
+std::vector<Block> best_partition(int n, const ketgpu_op* ops, const std::vector<int>& seg,
+                                  const PlanOptions& opt) {
+  std::vector<std::pair<int, int>> cands{{0, 0}};  // (0, 0): the program order
+  for (int w : kBandWidths)
+    for (int off = 0; off < w; ++off) cands.push_back({w, off});
+  const size_t C = cands.size();
+  std::vector<std::vector<Block>> parts(C);
+  std::vector<double> cost(C, 0.0);
+  auto work = [&](size_t c) {
+    const std::vector<int> order = cands[c].first ? band_order(ops, seg, n, cands[c].first, cands[c].second) : seg;
+    parts[c] = grow_blocks(n, ops, order, std::max(1, opt.max_k), true);
+    cost[c] = partition_cost(ops, parts[c], opt);
+  };
+  const unsigned nt = seg.size() < 256 ? 1u : std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+  if (nt <= 1) {
+    for (size_t c = 0; c < C; ++c) work(c);
+  } else {
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t)
+      th.emplace_back([&] {
+        for (size_t c; (c = next.fetch_add(1)) < C;) work(c);
+      });
+    for (auto& x : th) x.join();
+  }
+  size_t best = 0;
+  for (size_t c = 1; c < C; ++c)
+    if (cost[c] < cost[best] - 1e-9) best = c;
+  return std::move(parts[best]);
 }
 
 // ket's Fuser block rule on one barrier-free segment.
@@ -736,16 +773,7 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
     } else {
       // greedy growth over the program order and every band order; the
       // partition with the least static cost wins (the program order on ties)
-      std::vector<Block> best = grow_blocks(n, ops, seg, std::max(1, opt.max_k), true);
-      double best_cost = partition_cost(ops, best, opt);
-      for (int w : kBandWidths) {
-        std::vector<Block> cand = grow_blocks(n, ops, band_order(ops, seg, n, w), std::max(1, opt.max_k), true);
-        const double c = partition_cost(ops, cand, opt);
-        if (c < best_cost - 1e-9) {
-          best = std::move(cand);
-          best_cost = c;
-        }
-      }
+      std::vector<Block> best = best_partition(n, ops, seg, opt);
       for (const Block& b : best) {
         if (b.diag) {
           emit_diagonal(plan, n, ops, b);

@@ -122,7 +122,7 @@ def test_pass_qubits_describe_the_blocks():
             assert qs == []
         else:
             assert 1 <= len(qs) <= 3
-    assert n_tc == 117 and seen == set(range(30))
+    assert n_tc == 114 and seen == set(range(30))
     with pytest.raises(Exception):
         p.pass_qubits(10**6)
 
@@ -153,7 +153,7 @@ def test_tensor_core_producer_forms():
         else:
             with pytest.raises(ValueError):
                 p.pass_tc_form(i)
-    assert forms == {(2, True): 23, (3, True): 73, (4, True): 5, (0, False): 16}
+    assert forms == {(2, True): 21, (3, True): 68, (4, True): 9, (0, False): 16}
     # 4-qubit blocks (11-qubit tiles): the same rule
     p4 = Plan(30, random_brickwork(30, 40).to_ops(), ket.make_options("c64", "greedy", 4, True))
     for i in range(p4.stats()["n_passes"]):
@@ -343,10 +343,10 @@ def test_band_ordered_plans_apply_the_same_circuit(oracle, k):
 
 
 def test_band_orders_cut_the_brick_wall_passes():
-    """30 qubits x 40 layers: 154 passes in program order at k = 5 (round-1
-    plan), 119 with the band orders; at k = 6, 73."""
+    """30 qubits x 40 layers: 154 passes in program order at k = 5, 119 with
+    the band orders (every width 3..8 at every offset); at k = 6, 65."""
     import ket_b200 as ket
     from ket_b200.workloads import random_brickwork
     c = random_brickwork(30, 40)
     assert ket.plan_stats(c, ket.make_options("c64", "greedy", 5, True))["n_passes"] == 119
-    assert ket.plan_stats(c, ket.make_options("c64", "greedy", 6, True))["n_passes"] == 73
+    assert ket.plan_stats(c, ket.make_options("c64", "greedy", 6, True))["n_passes"] == 65
