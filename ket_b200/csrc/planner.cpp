@@ -673,8 +673,14 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
       // block taking its cheaper form.
       const int kmin_cand = std::min(3, std::max(1, opt.max_k));
       const int kmax_cap = std::max(kmin_cand, std::min(6, opt.max_k + 1));
+      // per k: the greedy partition of least static cost over the program
+      // order and the band orders (what FUSE_GREEDY would emit at that k)
       std::vector<std::vector<Block>> cands;
-      for (int kc = kmin_cand; kc <= kmax_cap; ++kc) cands.push_back(grow_blocks(n, ops, seg, kc, true));
+      for (int kc = kmin_cand; kc <= kmax_cap; ++kc) {
+        PlanOptions ok = opt;
+        ok.max_k = kc;
+        cands.push_back(best_partition(n, ops, seg, ok));
+      }
       std::vector<float> rows;
       float fr[kFeatures];
       // single-gate rows, one per gate of the segment
