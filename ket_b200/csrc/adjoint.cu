@@ -1324,7 +1324,7 @@ std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGat
   // store) beat one CTA with two buffers: the other CTA's work covers the
   // loads.  Forward: two CTAs, each prefetching its next tile.
   line("extern \"C\" __global__ void __launch_bounds__(256, 2)");
-  line("kb_tile_jit(float2* __restrict__ psi, float2* __restrict__ lam, uint64_t dim, kbt::TileGeom tg,");
+  line("kb_tile_jit(float2* psi, const float2* psi_src, float2* __restrict__ lam, uint64_t dim, kbt::TileGeom tg,");
   line("            const kbt::TGate* __restrict__ gates, int ngates, const float* __restrict__ mats,");
   line("            uint64_t mat_stride, int ngrad, double* __restrict__ partial) {");
   line("  using namespace kbt;");
@@ -1340,20 +1340,21 @@ std::string jit_source(const std::vector<TPhase>& phases, const std::vector<TGat
   line("  __shared__ uint64_t off_lo[64], off_hi[64];");
   line("  const int tid = threadIdx.x;");
   line("  const int set = blockIdx.y;");
-  line("  float2* s = psi + (uint64_t)set * dim;");
+  line("  float2* s = psi + (uint64_t)set * dim;  // tiles are stored here");
+  line("  const float2* sin = psi_src + (uint64_t)set * dim;  // and loaded from here (psi, or a checkpoint)");
   line("  float2* l = REV ? lam + (uint64_t)set * dim : nullptr;");
   line("  c64_setup<REV>(tg, gates, ngates, mats, mat_stride, set, GS ? kTileThreads * GS : 2 * kTileWarps * ngrad,");
   line("                 off_lo, off_hi, spk, accf);");
   line("  __syncthreads();");
   line("  int cur = 0;");
-  line("  if (!SINGLE && blockIdx.x < tg.n_tiles) c64_prefetch<REV>(tg, off_lo, off_hi, blockIdx.x, bufs, s, l);");
+  line("  if (!SINGLE && blockIdx.x < tg.n_tiles) c64_prefetch<REV>(tg, off_lo, off_hi, blockIdx.x, bufs, sin, l);");
   line("  asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");");
   line("  for (uint64_t t = blockIdx.x; t < tg.n_tiles; t += gridDim.x) {");
   line("    float2* sp = bufs + (SINGLE ? 0 : cur) * BUF;");
   line("    float2* sl = sp + TILE;");
-  line("    if (SINGLE) c64_prefetch<REV>(tg, off_lo, off_hi, t, bufs, s, l);");
+  line("    if (SINGLE) c64_prefetch<REV>(tg, off_lo, off_hi, t, bufs, sin, l);");
   line("    else if (t + gridDim.x < tg.n_tiles)");
-  line("      c64_prefetch<REV>(tg, off_lo, off_hi, t + gridDim.x, bufs + (cur ^ 1) * BUF, s, l);");
+  line("      c64_prefetch<REV>(tg, off_lo, off_hi, t + gridDim.x, bufs + (cur ^ 1) * BUF, sin, l);");
   line("    asm volatile(\"cp.async.commit_group;\\n\" ::: \"memory\");");
   line("    if (SINGLE) asm volatile(\"cp.async.wait_group 0;\\n\" ::: \"memory\");");
   line("    else asm volatile(\"cp.async.wait_group 1;\\n\" ::: \"memory\");");
@@ -1432,11 +1433,12 @@ std::atomic<uint64_t> g_jit_launches{0};
 template <typename R, bool REV>
 void launch_tile(dim3 grid, cudaStream_t st, typename C2T<R>::T* psi, typename C2T<R>::T* lam, uint64_t dim,
                  const TBlock& b, const TGate* gates, const TPhase* phases, const R* mats, uint64_t chunk,
-                 double* partial, cudaKernel_t jit = nullptr) {
+                 double* partial, cudaKernel_t jit = nullptr, const typename C2T<R>::T* psi_src = nullptr) {
   const int ngrad = REV ? (int)b.grad_gate.size() : 0;
   if constexpr (sizeof(R) == 4) {
     if (jit) {
       float2* a0 = psi;
+      const float2* asrc = psi_src ? psi_src : psi;
       float2* a1 = lam;
       uint64_t d = dim;
       TileGeom tg = b.geom;
@@ -1446,7 +1448,7 @@ void launch_tile(dim3 grid, cudaStream_t st, typename C2T<R>::T* psi, typename C
       uint64_t ms = chunk;
       int ngr = ngrad;
       double* pp = partial;
-      void* args[] = {&a0, &a1, &d, &tg, &gp, &ng, &mp, &ms, &ngr, &pp};
+      void* args[] = {&a0, &asrc, &a1, &d, &tg, &gp, &ng, &mp, &ms, &ngr, &pp};
       KB_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(jit), grid, dim3(kTileThreads), args,
                                jit_smem(REV, b.n_gates, ngrad), st));
       count_launch();
@@ -1454,6 +1456,8 @@ void launch_tile(dim3 grid, cudaStream_t st, typename C2T<R>::T* psi, typename C
       return;
     }
   }
+  if (psi_src && psi_src != psi)  // the interpreted sweeps load in place only
+    KB_CUDA(cudaMemcpyAsync(psi, psi_src, dim * sizeof(typename C2T<R>::T) * grid.y, cudaMemcpyDeviceToDevice, st));
   const size_t smem = tile_smem<R>(REV, b.n_gates, ngrad);
   if constexpr (sizeof(R) == 4)
     tile_sweep_c64<REV><<<grid, kTileThreads, smem, st>>>(psi, lam, dim, b.geom, gates + b.gate_first, b.n_gates,
@@ -1703,9 +1707,17 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
       for (size_t i = 0; i < hmats.size(); ++i) hmats_t[i] = (R)hmats[i];
       KB_CUDA(cudaMemcpyAsync(mats_t.p, hmats_t.data(), sizeof(R) * hmats_t.size(), cudaMemcpyHostToDevice, st));
     }
+    // With every block compiled, checkpoints cost no copies: the block
+    // before a checkpoint writes its tiles into the checkpoint, the next
+    // block reads them from there and writes psi (and in the reverse sweep
+    // the first block of a segment reads psi from its checkpoint).
+    bool ck_direct = tiled && !jit_fwd.empty();
+    for (size_t bi = 0; ck_direct && bi < jit_fwd.size(); ++bi) ck_direct = jit_fwd[bi] && jit_rev[bi];
+    auto ck_at = [&](int k) { return ck.as<T>() + (size_t)k * chunk * dim; };
     // forward
-    KB_CUDA(cudaMemsetAsync(psi.p, 0, dim * sizeof(T) * nb, st));
-    ground_batch<R><<<(unsigned)nb, 1, 0, st>>>(psi.as<T>(), dim);
+    T* ground = ck_direct ? ck_at(0) : psi.as<T>();
+    KB_CUDA(cudaMemsetAsync(ground, 0, dim * sizeof(T) * nb, st));
+    ground_batch<R><<<(unsigned)nb, 1, 0, st>>>(ground, dim);
     count_launch();
     // checkpoint k = the state at the start of layer k*m
     int next_ck = 0;
@@ -1714,7 +1726,28 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
                               cudaMemcpyDeviceToDevice, st));
       ++next_ck;
     };
-    if (tiled) {
+    if (ck_direct) {
+      const int B = (int)tp.blocks.size();
+      const T* cur = ground;  // where the state lives now
+      next_ck = 1;            // checkpoint 0 is the ground state
+      for (int bi = 0; bi < B; ++bi) {
+        const TBlock& b = tp.blocks[bi];
+        if (cur != psi.as<T>() && next_ck < n_ckpt && next_ck * m <= b.layer) {
+          // more checkpoints due here than blocks between them
+          KB_CUDA(cudaMemcpyAsync(psi.p, cur, dim * sizeof(T) * nb, cudaMemcpyDeviceToDevice, st));
+          cur = psi.as<T>();
+        }
+        while (cur == psi.as<T>() && next_ck < n_ckpt && next_ck * m <= b.layer) store_ck();
+        T* out = psi.as<T>();
+        if (bi + 1 < B && next_ck < n_ckpt && next_ck * m <= tp.blocks[bi + 1].layer) out = ck_at(next_ck++);
+        dim3 grid((unsigned)gx, (unsigned)nb);
+        launch_tile<R, false>(grid, st, out, nullptr, dim, b, d_tgates->as<TGate>(), d_tphases->as<TPhase>(),
+                              mats_t.as<R>(), chunk, nullptr, jit_fwd[bi], cur);
+        cur = out;
+      }
+      if (cur != psi.as<T>())
+        KB_CUDA(cudaMemcpyAsync(psi.p, cur, dim * sizeof(T) * nb, cudaMemcpyDeviceToDevice, st));
+    } else if (tiled) {
       for (const TBlock& b : tp.blocks) {
         while (next_ck < n_ckpt && next_ck * m <= b.layer) store_ck();
         dim3 grid((unsigned)gx, (unsigned)nb);
@@ -1764,13 +1797,17 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
       for (int bi = B; bi-- > 0;) {
         const TBlock& b = tp.blocks[bi];
         const int seg = b.layer / m;
-        if (bi + 1 < B && tp.blocks[bi + 1].layer / m != seg && seg + 1 < n_ckpt)
-          KB_CUDA(cudaMemcpyAsync(psi.p, ck.as<T>() + (size_t)(seg + 1) * chunk * dim, dim * sizeof(T) * nb,
-                                  cudaMemcpyDeviceToDevice, st));
+        const T* src = psi.as<T>();
+        if (bi + 1 < B && tp.blocks[bi + 1].layer / m != seg && seg + 1 < n_ckpt) {
+          if (ck_direct) src = ck_at(seg + 1);
+          else
+            KB_CUDA(cudaMemcpyAsync(psi.p, ck.as<T>() + (size_t)(seg + 1) * chunk * dim, dim * sizeof(T) * nb,
+                                    cudaMemcpyDeviceToDevice, st));
+        }
         dim3 grid((unsigned)gx, (unsigned)nb);
         launch_tile<R, true>(grid, st, psi.as<T>(), lam.as<T>(), dim, b, d_tgates->as<TGate>(),
                              d_tphases->as<TPhase>(), mats_t.as<R>(), chunk, part.as<double>() + b.part_off,
-                             jit_rev.empty() ? nullptr : jit_rev[bi]);
+                             jit_rev.empty() ? nullptr : jit_rev[bi], src);
       }
     } else {
       for (size_t gi = G; gi-- > 0;) {
