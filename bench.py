@@ -253,15 +253,15 @@ def run_sample33(args):
     plan.close()
 
 
-def _adjoint_blocks(n, ops, pidx):
+def _adjoint_blocks(n, ops, pidx, ckpt):
     """Number of tile blocks of the tiled adjoint sweep (complex64)."""
     from ket_b200 import _lib
     p = np.ascontiguousarray(pidx, dtype=np.int32)
     length = ct.c_uint64()
-    _lib.check(_lib.lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), p.ctypes.data, _lib.C64, None, 0,
-                                                     ct.byref(length)))
+    _lib.check(_lib.lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), p.ctypes.data, _lib.C64, ckpt,
+                                                     None, 0, ct.byref(length)))
     out = np.zeros(length.value, dtype=np.int32)
-    _lib.check(_lib.lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), p.ctypes.data, _lib.C64,
+    _lib.check(_lib.lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), p.ctypes.data, _lib.C64, ckpt,
                                                      out.ctypes.data, length.value, ct.byref(length)))
     return int(out[0])
 
@@ -290,7 +290,7 @@ def run_adjoint24(args):
     # algorithmic HBM bytes per batch: per tile block and set, the forward
     # reads and writes psi, the reverse psi and lambda; lambda = H psi reads
     # psi and writes lambda once per set (its gathers beyond that are L2 hits)
-    blocks = _adjoint_blocks(n, circ.to_ops(), pidx)
+    blocks = _adjoint_blocks(n, circ.to_ops(), pidx, 2)
     state = 8 * 2 ** n
     byts = batch * (blocks * (2 * state + 4 * state) + 2 * state)
     peak, peak_kind = peaks()

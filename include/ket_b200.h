@@ -288,16 +288,18 @@ int ketgpu_adjoint_ex(int32_t n_qubits, const ketgpu_op* ops, uint64_t n_ops,
                       const char* const* paulis, uint64_t n_terms,
                       int32_t precision, int32_t checkpoint_every,
                       int32_t method, double* values, double* grads);
-/* The tiled sweeps' plan as flat int32 records (layout documented in
- * ket_b200/csrc/adjoint.cu); *length receives the record count, out may be
- * NULL to query it. */
 /* NVRTC availability, distinct per-block kernels compiled so far, and
  * launches that used one. */
 int ketgpu_adjoint_jit_info(int32_t* available, uint64_t* kernels, uint64_t* launches);
+/* The tiled sweeps' plan as flat int32 records (layout documented in
+ * ket_b200/csrc/adjoint.cu) for the given checkpoint interval (blocks may
+ * run across the barrier-delimited layers of one checkpoint segment, never
+ * across its ends); *length receives the record count, out may be NULL to
+ * query it. */
 int ketgpu_adjoint_plan_describe(int32_t n_qubits, const ketgpu_op* ops,
                                  uint64_t n_ops, const int32_t* param_index,
-                                 int32_t precision, int32_t* out,
-                                 uint64_t capacity, uint64_t* length);
+                                 int32_t precision, int32_t checkpoint_every,
+                                 int32_t* out, uint64_t capacity, uint64_t* length);
 
 /* ---- learned fusion cost model (48 -> 128 -> 128 -> 1 MLP, BF16 weights,
  *      FP32 accumulation; no ket counterpart) ------------------------- */

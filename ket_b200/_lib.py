@@ -99,7 +99,7 @@ def _load():
         "ketgpu_sample_tree_builds": ([], u64),
         "ketgpu_adjoint": ([i32, vp, u64, vp, vp, u64, u64, vp, vp, u64, i32, i32, vp, vp], ct.c_int),
         "ketgpu_adjoint_ex": ([i32, vp, u64, vp, vp, u64, u64, vp, vp, u64, i32, i32, i32, vp, vp], ct.c_int),
-        "ketgpu_adjoint_plan_describe": ([i32, vp, u64, vp, i32, vp, u64, vp], ct.c_int),
+        "ketgpu_adjoint_plan_describe": ([i32, vp, u64, vp, i32, i32, vp, u64, vp], ct.c_int),
         "ketgpu_adjoint_jit_info": ([vp, vp, vp], ct.c_int),
         "ketgpu_mlp_create": ([u64, ct.POINTER(vp)], ct.c_int),
         "ketgpu_mlp_destroy": ([vp], ct.c_int),

@@ -993,7 +993,7 @@ TileOp tile_op_of(const Pass& p, const int* tpos_of_qubit) {
 
 template <typename R>
 TilePlan plan_tiles(int n, const ketgpu_op* ops, const std::vector<int>& gate_ops, const std::vector<int>& layer_of,
-                    const std::vector<GateGeom>& geo, const std::vector<uint8_t>& real) {
+                    const std::vector<GateGeom>& geo, const std::vector<uint8_t>& real, int seg_layers) {
   constexpr int TB = TileCfg<R>::TB, RB = TileCfg<R>::RB;
   constexpr bool kPacked = sizeof(R) == 4;  // complex64 sweeps pack pairs of amplitudes
   TilePlan tp;
@@ -1007,8 +1007,10 @@ TilePlan plan_tiles(int n, const ketgpu_op* ops, const std::vector<int>& gate_op
   }
   int i0 = 0;
   while (i0 < G) {
+    // one checkpoint segment (seg_layers layers) at a time: blocks may run
+    // across the layers of a segment but never across its ends
     int i1 = i0;
-    while (i1 < G && layer_of[i1] == layer_of[i0]) ++i1;
+    while (i1 < G && layer_of[i1] / seg_layers == layer_of[i0] / seg_layers) ++i1;
     // A topological order of the layer that sweeps the qubits upwards: among
     // the gates whose predecessors (earlier gates sharing a qubit) are
     // placed, take the one with the lowest highest qubit.  Chains such as a
@@ -1174,6 +1176,20 @@ TilePlan plan_tiles(int n, const ketgpu_op* ops, const std::vector<int>& gate_op
     i0 = i1;
   }
   return tp;
+}
+
+// The tiled plan with blocks per layer, or per checkpoint segment of m
+// layers when that needs fewer blocks (fewer HBM passes; a block that spans
+// layers holds more gates and register phases, so on a tie the per-layer
+// plan is kept).
+template <typename R>
+TilePlan plan_tiles_best(int n, const ketgpu_op* ops, const std::vector<int>& gate_ops,
+                         const std::vector<int>& layer_of, const std::vector<GateGeom>& geo,
+                         const std::vector<uint8_t>& real, int m) {
+  TilePlan per_layer = plan_tiles<R>(n, ops, gate_ops, layer_of, geo, real, 1);
+  if (m <= 1) return per_layer;
+  TilePlan per_seg = plan_tiles<R>(n, ops, gate_ops, layer_of, geo, real, m);
+  return per_seg.blocks.size() < per_layer.blocks.size() ? std::move(per_seg) : std::move(per_layer);
 }
 
 struct DevBuf {
@@ -1628,7 +1644,7 @@ void run_adjoint(int n, const ketgpu_op* ops, uint64_t nops, const int32_t* pidx
         if (d[1] != 0.0 || d[3] != 0.0 || d[5] != 0.0 || d[7] != 0.0) real[gi] = 0;
         if (geo[gi].pslot < 0) break;  // the same matrix for every set
       }
-    tp = plan_tiles<R>(n, ops, gate_ops, layer_of, geo, real);
+    tp = plan_tiles_best<R>(n, ops, gate_ops, layer_of, geo, real, m);
     d_tgates = std::make_unique<DevBuf>(sizeof(TGate) * std::max<size_t>(tp.gates.size(), 1));
     d_tphases = std::make_unique<DevBuf>(sizeof(TPhase) * std::max<size_t>(tp.phases.size(), 1));
     if (!tp.gates.empty())
@@ -1922,8 +1938,8 @@ KB_API int ketgpu_adjoint_ex(int32_t n, const ketgpu_op* ops, uint64_t n_ops, co
 // phase.first relative to the block's first gate.  Angles are taken from
 // the ops as given (the real flag is per those angles).
 KB_API int ketgpu_adjoint_plan_describe(int32_t n, const ketgpu_op* ops, uint64_t n_ops,
-                                        const int32_t* param_index, int32_t precision, int32_t* out,
-                                        uint64_t capacity, uint64_t* length) {
+                                        const int32_t* param_index, int32_t precision, int32_t checkpoint_every,
+                                        int32_t* out, uint64_t capacity, uint64_t* length) {
   try {
     if (!ops || !length) fail(KETGPU_ERR_INVALID, "adjoint_plan_describe: null argument");
     validate_ops(n, ops, n_ops);
@@ -1952,8 +1968,9 @@ KB_API int ketgpu_adjoint_plan_describe(int32_t n, const ketgpu_op* ops, uint64_
       for (int j = 0; j < 4; ++j) r = r && p.m[j].imag() == 0.0;
       real[gi] = r && p.kind == PassKind::Pair;
     }
-    const TilePlan tp = precision == KETGPU_C64 ? plan_tiles<float>(n, ops, gate_ops, layer_of, geo, real)
-                                                : plan_tiles<double>(n, ops, gate_ops, layer_of, geo, real);
+    const int m = checkpoint_every > 0 ? checkpoint_every : layer + 1;
+    const TilePlan tp = precision == KETGPU_C64 ? plan_tiles_best<float>(n, ops, gate_ops, layer_of, geo, real, m)
+                                                : plan_tiles_best<double>(n, ops, gate_ops, layer_of, geo, real, m);
     std::vector<int32_t> v;
     v.push_back((int32_t)tp.blocks.size());
     for (const TBlock& b : tp.blocks) {

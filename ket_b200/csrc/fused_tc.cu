@@ -261,7 +261,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __shared__ __align__(8) uint64_t bar_full[S], bar_free[S];
   __shared__ __align__(8) uint64_t bar_a_ready[2], bar_mma[2], bar_acc_free[2];
   __shared__ uint32_t tmem_base_slot;
-  __shared__ uint64_t base_ring[2 * S];
+  // Tile bases, written by the producer when it issues a tile and read by
+  // the epilogue once the tile's MMAs are done.  The producer can run at
+  // most 2S tiles ahead of the direct epilogue (k <= 5: it waits for a slot
+  // that the converters free only after MMAs that wait for the epilogue of
+  // four tiles back), and 3 with one slot (k = 6); R entries cover both.
+  constexpr int R = 2 * S > 8 ? 2 * S : 8;
+  __shared__ uint64_t base_ring[R];
   __shared__ volatile int abort_flag;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -378,7 +384,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int slot = (int)(j % S);
         if (j >= (uint64_t)S && !wait(&bar_free[slot], (uint32_t)(((j / S) - 1) & 1))) break;
         const uint64_t base = tile_base(first + j * stride);
-        base_ring[j % (2 * S)] = base;
+        base_ring[j % R] = base;
         const uint32_t bar = smem_u32(&bar_full[slot]);
         mbar_arrive_expect_tx(bar, (uint32_t)Cfg::RAW_BYTES);
         int crd[5];
@@ -427,7 +433,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&bar_full[slot]))
                    : "memory");
       if (tid == 0) {
-        base_ring[j % (2 * S)] = base;
+        base_ring[j % R] = base;
         arrive(&bar_full[slot]);
       }
     }
@@ -521,7 +527,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
       bool ok = true;
       for (uint64_t j = 0; j < count && ok; ++j) {
-        float2* dst = s + base_ring[j % (2 * S)] + gdep;
+        float2* dst = nullptr;
         for (int h = 0; h < Cfg::PASSES; ++h) {
           const uint64_t u = j * Cfg::PASSES + h;  // accumulator use: region u%2, its (u/2)-th
           if (!wait(&bar_mma[u & 1], (uint32_t)((u >> 1) & 1))) {
@@ -529,6 +535,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             break;
           }
           tc_fence_after();
+          // tile j's base is in the ring once its MMAs are done (the
+          // producer wrote it before the tile's copy was even issued)
+          if (h == 0) dst = s + base_ring[j % R] + gdep;
           const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS) +
                                ((uint32_t)(32 * q) << 16);
 #pragma unroll
@@ -587,7 +596,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
       if (!ok) break;
       asm volatile("bar.sync 1, %0;" ::"n"(kEpilogue) : "memory");
-      float2* dst = s + base_ring[j % (2 * S)];
+      float2* dst = s + base_ring[j % R];
 #pragma unroll
       for (int i = 0; i < CPT; ++i)
         *reinterpret_cast<float4*>(dst + goff[i]) = *reinterpret_cast<const float4*>(out + soff[i]);

@@ -19,7 +19,7 @@ TILE = {"c64": (12, 4), "c128": (11, 3)}
 NTHREADS = 256
 
 
-def _describe(n, ops, pidx, prec):
+def _describe(n, ops, pidx, prec, ckpt=1):
     import ctypes as ct
 
     from ket_b200 import _lib
@@ -27,10 +27,10 @@ def _describe(n, ops, pidx, prec):
     pid = np.ascontiguousarray(pidx, dtype=np.int32)
     length = ct.c_uint64()
     p = _lib.C64 if prec == "c64" else _lib.C128
-    _lib.check(lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), pid.ctypes.data, p, None, 0,
+    _lib.check(lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), pid.ctypes.data, p, ckpt, None, 0,
                                                 ct.byref(length)))
     out = np.zeros(length.value, dtype=np.int32)
-    _lib.check(lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), pid.ctypes.data, p,
+    _lib.check(lib.ketgpu_adjoint_plan_describe(n, ops.ctypes.data, len(ops), pid.ctypes.data, p, ckpt,
                                                 out.ctypes.data, length.value, ct.byref(length)))
     v = list(out)
     k = 0
@@ -217,10 +217,17 @@ def _random_circuit(n, count, seed, barriers=3):
     return make_ops(gs), np.array(pidx, dtype=np.int32), k
 
 
+@pytest.mark.parametrize("ckpt", [1, 2, 0])
 @pytest.mark.parametrize("prec,n,seed", [("c128", 11, 1), ("c128", 13, 2), ("c64", 12, 3), ("c64", 14, 4)])
-def test_tiled_plan_reproduces_the_oracle(oracle, prec, n, seed):
+def test_tiled_plan_reproduces_the_oracle(oracle, prec, n, seed, ckpt):
+    """ckpt: the checkpoint interval in barrier-delimited layers; with more
+    than one layer per segment, blocks may run across a segment's layers."""
     ops, pidx, npar = _random_circuit(n, 90, seed)
-    blocks = _describe(n, ops, pidx, prec)
+    blocks = _describe(n, ops, pidx, prec, ckpt)
+    if ckpt == 1:  # one layer per block
+        layer_of = np.cumsum([o["type"] == CODE["Barrier"] for o in ops])
+        for b in blocks:
+            assert {int(layer_of[g["op"]]) for g in b["gates"]} == {b["layer"]}
     if prec == "c64":
         # complex64 phases keep register slot 0 for the pack bit: no pair gate
         # targets it and no gate uses it as a control
@@ -283,3 +290,16 @@ def test_ansatz_layer_needs_three_tiles_at_24_qubits():
     blocks = _describe(24, circ.to_ops(), pidx, "c64")
     assert len(blocks) == 6
     assert all(len(b["phases"]) <= 4 for b in blocks)
+
+
+def test_ansatz_blocks_span_layers_only_when_that_saves_passes():
+    """20 qubits, 8 layers, checkpoints every 2 layers: blocks that run
+    across the two layers of a segment need 20 passes instead of 24; at 24
+    qubits they would save none, and the per-layer plan is kept."""
+    from ket_b200.workloads import variational_ansatz
+    circ, pidx = variational_ansatz(20, 8)
+    assert len(_describe(20, circ.to_ops(), pidx, "c64", 1)) == 24
+    assert len(_describe(20, circ.to_ops(), pidx, "c64", 2)) == 20
+    circ, pidx = variational_ansatz(24, 8)
+    b2 = _describe(24, circ.to_ops(), pidx, "c64", 2)
+    assert len(b2) == 24 and max(len(b["phases"]) for b in b2) <= 4
