@@ -73,9 +73,19 @@ struct TcCfg {
   // staging images: as many as fit next to the B images (loads in flight)
   static constexpr int SLOTS_FIT = (kSmemBudget - 1024 - 2 * B_BYTES) / RAW_BYTES;
   static constexpr int SLOTS = SLOTS_FIT > 12 ? 12 : SLOTS_FIT;
-  static constexpr size_t SMEM = (size_t)SLOTS * RAW_BYTES + 2 * B_BYTES + 1024;  // + alignment slack
+  // k = 6 with a tensor copy: half-tile staging slots (the tile split by its
+  // highest target qubit), so copies run ahead of the split
+  static constexpr int HALF_BYTES = RAW_BYTES / 2;
+  static constexpr int HSLOTS = SPLIT ? (kSmemBudget - 1024 - 2 * B_BYTES) / HALF_BYTES : 0;
+  static constexpr int SB = SLOTS > HSLOTS ? SLOTS : HSLOTS;  // barrier pairs
+  static constexpr size_t STAGE = (size_t)SLOTS * RAW_BYTES > (size_t)HSLOTS * HALF_BYTES
+                                      ? (size_t)SLOTS * RAW_BYTES
+                                      : (size_t)HSLOTS * HALF_BYTES;
+  static constexpr size_t SMEM = STAGE + 2 * B_BYTES + 1024;  // + alignment slack
   static_assert(TMEM_COLS <= 512 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory budget");
   static_assert(SLOTS >= (SPLIT ? 1 : 3), "shared memory budget");
+  static_assert(!SPLIT || HSLOTS >= 3, "shared memory budget");
+  static_assert(SMEM <= (size_t)kSmemBudget + 1024, "shared memory budget");
 };
 
 struct TcGeom {
@@ -95,6 +105,13 @@ struct TcGeom {
   uint32_t ctile[64];
   uint64_t cdep[64];  // offset of target combination c from its group's amplitude
   uint64_t n_tiles;
+  // k = 6 tensor copy in half tiles (half = 1): each tile is two boxes of
+  // the tensor map over the tile less its highest target qubit, at the tile
+  // base and at base + top_off; ctile[0..31] are the low five targets'
+  // offsets in a half box and gbit_off[b] is group bit b's.
+  int half;
+  uint64_t top_off;
+  uint32_t gbit_off[kGroupBits];
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -258,7 +275,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   unsigned char* b_lo = b_hi + Cfg::B_BYTES;
   unsigned char* raw = b_lo + Cfg::B_BYTES;
 
-  __shared__ __align__(8) uint64_t bar_full[S], bar_free[S];
+  constexpr int SB = Cfg::SB;
+  constexpr int HS = Cfg::HSLOTS > 0 ? Cfg::HSLOTS : 1;
+  __shared__ __align__(8) uint64_t bar_full[SB], bar_free[SB];
   __shared__ __align__(8) uint64_t bar_a_ready[2], bar_mma[2], bar_acc_free[2];
   __shared__ uint32_t tmem_base_slot;
   // Tile bases, written by the producer when it issues a tile and read by
@@ -273,7 +292,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (tid == 0) {
-    for (int i = 0; i < S; ++i) {
+    for (int i = 0; i < SB; ++i) {
       mbar_init(smem_u32(&bar_full[i]), g.tma_dims ? 1 : kProducers + 1);
       mbar_init(smem_u32(&bar_free[i]), kEpilogue);
     }
@@ -372,7 +391,45 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     return b;
   };
 
-  if (warp < 4 && g.tma_dims) {
+  if (Cfg::SPLIT && warp < 4 && g.half) {
+    // ------------------------------- producer, k = 6 tensor copy in halves
+    // Half q = 2j + h of tile j (h: the highest target's bit) goes to slot
+    // q % HS; three slots let the copies run a tile and a half ahead.
+    if (tid == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap)) : "memory");
+      uint64_t issued = 0;
+      for (uint64_t q = 0; q < 2 * count; ++q) {
+        const uint64_t j = q >> 1;
+        const int slot = (int)(q % HS);
+        if (q >= (uint64_t)HS && !wait(&bar_free[slot], (uint32_t)(((q / HS) - 1) & 1))) break;
+        uint64_t base = tile_base(first + j * stride);
+        if ((q & 1) == 0) base_ring[j % R] = base;
+        else base |= g.top_off;
+        const uint32_t bar = smem_u32(&bar_full[slot]);
+        mbar_arrive_expect_tx(bar, (uint32_t)Cfg::HALF_BYTES);
+        int crd[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) crd[i] = (int)((base >> g.tma_start[i]) & g.tma_mask[i]);
+        tma_load_box(smem_u32(raw + slot * Cfg::HALF_BYTES), &tmap, crd, g.tma_dims, bar);
+        issued = q + 1;
+      }
+      // drain: every issued copy lands before the CTA may leave
+      for (uint64_t q = issued > (uint64_t)HS ? issued - HS : 0; q < issued; ++q) {
+        const uint32_t a = smem_u32(&bar_full[q % HS]);
+        for (uint32_t it = 0; it < kWaitLimit; ++it) {
+          uint32_t done;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+              "selp.u32 %0, 1, 0, p;\n\t}"
+              : "=r"(done)
+              : "r"(a), "r"((uint32_t)((q / HS) & 1))
+              : "memory");
+          if (done) break;
+        }
+      }
+    }
+  } else if (warp < 4 && g.tma_dims) {
     // ------------------------------------------ producer, tensor-copy form
     // One thread fetches each whole tile with a single tiled tensor copy;
     // the image holds the tile in its natural index order under the
@@ -438,6 +495,56 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (Cfg::SPLIT && warp < 8 && g.half) {
+    // --------------------------------- converters, k = 6 tensor copy in halves
+    // As below, with the row read from two half boxes: half h holds the
+    // combinations whose highest target bit is h, i.e. A columns 64h..64h+63.
+    const int q4 = warp & 3;
+    const int lane_row = 32 * q4 + lane;
+    const uint32_t lane_off = (uint32_t)(32 * q4) << 16;
+    uint32_t gtile = 0;
+#pragma unroll
+    for (int b = 0; b < kGroupBits; ++b)
+      if ((lane_row >> b) & 1) gtile |= g.gbit_off[b];
+    bool ok = true;
+    for (uint64_t j = 0; j < count && ok; ++j) {
+      if (j >= 1 && !wait(&bar_mma[1], (uint32_t)((j - 1) & 1))) break;  // A region free
+      tc_fence_after();
+      const uint32_t areg = tmem + lane_off;
+      for (int h = 0; h < 2; ++h) {
+        const uint64_t q = 2 * j + h;
+        const int slot = (int)(q % HS);
+        if (!wait(&bar_full[slot], (uint32_t)((q / HS) & 1))) {
+          ok = false;
+          break;
+        }
+        const unsigned char* img = raw + slot * Cfg::HALF_BYTES;
+#pragma unroll
+        for (int part = 0; part < K / 32; ++part) {
+          uint32_t hi[16], lo[16], xs[16];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const uint32_t off = g.ctile[part * 8 + i] | gtile;
+            const uint2 x = *reinterpret_cast<const uint2*>(img + (off ^ ((off >> 3) & 0x70u)));
+            xs[2 * i] = x.x;
+            xs[2 * i + 1] = x.y;
+          }
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            const uint32_t hh = (xs[u] + 0x1000u) & 0xffffe000u;
+            hi[u] = hh;
+            lo[u] = (__float_as_uint(__uint_as_float(xs[u]) - __uint_as_float(hh)) + 0x1000u) & 0xffffe000u;
+          }
+          tmem_st16(areg + (uint32_t)(h * (K / 2) + part * 16), hi);
+          tmem_st16(areg + (uint32_t)(K + h * (K / 2) + part * 16), lo);
+        }
+        arrive(&bar_free[slot]);  // the direct epilogue never reads the image
+      }
+      if (!ok) break;
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      tc_fence_before();
+      arrive(&bar_a_ready[0]);
+    }
   } else if (warp < 8) {
     // ----------------------------------------------------------- converters
     // Thread = A row (TMEM lane 32*(warp%4) + lane): read the row from the
@@ -836,6 +943,59 @@ void tile_geometry(int n, const Pass& p, TcGeom& g) {
   g.n_tiles = (uint64_t{1} << n) >> Cfg::TB;
 }
 
+// The half tile of a k = 6 block (host only): the tile less its highest
+// target qubit `top`, as a 12-bit tile geometry.
+void half_geometry(const TcGeom& g, int tb, int top, TcGeom& hg) {
+  hg = g;
+  int j = 0;
+  for (int i = 0; i < tb; ++i)
+    if (g.tile_pos[i] != top) {
+      hg.tile_pos[j] = g.tile_pos[i];
+      hg.is_target[j] = g.is_target[i];
+      ++j;
+    }
+  for (; j < 16; ++j) hg.tile_pos[j] = hg.is_target[j] = 0;
+}
+
+// k = 6: whether the block takes the tensor copy in half tiles, and the
+// half tiles' map, offsets and coordinates in g (host only).
+int encode_half_tiles(const State* st, const Pass& p, TcGeom& g, CUtensorMap* map) {
+  constexpr int TBH = 6 + kGroupBits - 1;
+  TcGeom hg;
+  half_geometry(g, TBH + 1, p.qubits[5], hg);
+  Pass p5 = p;
+  p5.k = 5;
+  if (!tma_wanted(hg, p5, TBH)) return 0;
+  int nd;
+  if (st) {
+    nd = encode_tile_map(*st, hg, TBH, map);
+  } else {
+    int start[16], tq[16];
+    nd = tile_runs(hg, TBH, start, tq);
+  }
+  if (!nd) return 0;
+  g.tma_dims = nd;
+  g.half = 1;
+  g.top_off = uint64_t{1} << p.qubits[5];
+  g.direct = 1;
+  for (int i = 0; i < 5; ++i) {
+    g.tma_start[i] = hg.tma_start[i];
+    g.tma_mask[i] = hg.tma_mask[i];
+  }
+  for (int c = 0; c < 32; ++c) {
+    uint32_t off = 0;
+    for (int b = 0, jb = 0; jb < TBH; ++jb)
+      if (hg.is_target[jb]) {
+        if ((c >> b) & 1) off |= 8u << jb;
+        ++b;
+      }
+    g.ctile[c] = off;
+  }
+  for (int b = 0, jb = 0; jb < TBH; ++jb)
+    if (!hg.is_target[jb]) g.gbit_off[b++] = 8u << jb;
+  return nd;
+}
+
 template <int KQ>
 void launch_tc(const State& st, const Pass& p, const void* b_image) {
   using Cfg = TcCfg<KQ>;
@@ -844,8 +1004,12 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   CUtensorMap tmap;
   std::memset(&tmap, 0, sizeof(tmap));
   // Tensor-copy blocks (qubit 0 a group bit) always store directly.
-  g.tma_dims = tma_wanted(g, p, Cfg::TB) ? encode_tile_map(st, g, Cfg::TB, &tmap) : 0;
-  if (g.tma_dims) {
+  if constexpr (KQ == 6) {
+    g.tma_dims = encode_half_tiles(&st, p, g, &tmap);
+  } else {
+    g.tma_dims = tma_wanted(g, p, Cfg::TB) ? encode_tile_map(st, g, Cfg::TB, &tmap) : 0;
+  }
+  if (g.tma_dims && !g.half) {
     g.direct = 1;
     for (int c = 0; c < Cfg::DIM; ++c) {
       uint32_t off = 0;
@@ -932,7 +1096,9 @@ void tc_form(int n, const Pass& p, int* tma_dims, int* direct) {
   else if (p.k == 6) tile_geometry<6>(n, p, g);
   else tile_geometry<4>(n, p, g);
   int start[16], tq[16];
-  const int nd = tma_wanted(g, p, p.k + kGroupBits) ? tile_runs(g, p.k + kGroupBits, start, tq) : 0;
+  const int nd = p.k == 6 ? encode_half_tiles(nullptr, p, g, nullptr)
+                 : tma_wanted(g, p, p.k + kGroupBits) ? tile_runs(g, p.k + kGroupBits, start, tq)
+                                                       : 0;
   *tma_dims = nd;
   *direct = nd ? 1 : g.direct;
 }

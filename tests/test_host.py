@@ -350,3 +350,32 @@ def test_band_orders_cut_the_brick_wall_passes():
     c = random_brickwork(30, 40)
     assert ket.plan_stats(c, ket.make_options("c64", "greedy", 5, True))["n_passes"] == 119
     assert ket.plan_stats(c, ket.make_options("c64", "greedy", 6, True))["n_passes"] == 65
+
+
+def test_six_qubit_blocks_copy_half_tiles():
+    """k = 6 blocks whose qubit 0 is a group bit fetch each tile as two tensor
+    copies of half a tile (split by the highest target), so three 32 KB
+    staging slots fit beside the 128 KB of B images; blocks on qubit 0 keep
+    the single 64 KB cp.async slot."""
+    import collections
+    import ket_b200 as ket
+    from ket_b200.api import Plan
+    from ket_b200.workloads import random_brickwork
+    p = Plan(30, random_brickwork(30, 40).to_ops(), ket.make_options("c64", "greedy", 6, True))
+    forms = collections.Counter()
+    for i in range(p.stats()["n_passes"]):
+        info = p.pass_info(i)
+        if info["kind"] == 2 and info["tensor"]:
+            f = p.pass_tc_form(i)
+            forms[(info["k"], f["tma_dims"] > 0, f["direct"])] += 1
+    assert forms == {(6, True, True): 56, (6, False, False): 7}
+    for qs, want in {(2, 3, 4, 5, 6, 7): 3, (1, 3, 5, 7, 9, 11): 3, (10, 11, 12, 13, 14, 15): 3,
+                     (0, 1, 2, 3, 4, 5): 0}.items():
+        c = ket.Circuit(28)
+        for q in qs:
+            c.u(q, 0.3, 0.2, 0.1)
+        for a, b in zip(qs[:-1], qs[1:]):
+            c.cx(a, b)
+        pp = Plan(28, c.to_ops(), ket.make_options("c64", "greedy", 6, True))
+        tc = [i for i in range(pp.stats()["n_passes"]) if pp.pass_info(i)["tensor"]]
+        assert pp.pass_tc_form(tc[0])["tma_dims"] == want, qs
