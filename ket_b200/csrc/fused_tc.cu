@@ -279,6 +279,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   constexpr int HS = Cfg::HSLOTS > 0 ? Cfg::HSLOTS : 1;
   __shared__ __align__(8) uint64_t bar_full[SB], bar_free[SB];
   __shared__ __align__(8) uint64_t bar_a_ready[2], bar_mma[2], bar_acc_free[2];
+  // k = 6: bar_a_ready[k] / bar_a_free[k] hand K-half k of the one A region
+  // (A columns 64k..64k+63 and their lo copy) between converters and MMAs
+  __shared__ __align__(8) uint64_t bar_a_free[2];
   __shared__ uint32_t tmem_base_slot;
   // Tile bases, written by the producer when it issues a tile and read by
   // the epilogue once the tile's MMAs are done.  The producer can run at
@@ -300,6 +303,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(smem_u32(&bar_a_ready[i]), kConverters);
       mbar_init(smem_u32(&bar_mma[i]), 1);
       mbar_init(smem_u32(&bar_acc_free[i]), kEpilogue);
+      mbar_init(smem_u32(&bar_a_free[i]), 1);
     }
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -508,16 +512,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if ((lane_row >> b) & 1) gtile |= g.gbit_off[b];
     bool ok = true;
     for (uint64_t j = 0; j < count && ok; ++j) {
-      if (j >= 1 && !wait(&bar_mma[1], (uint32_t)((j - 1) & 1))) break;  // A region free
-      tc_fence_after();
       const uint32_t areg = tmem + lane_off;
       for (int h = 0; h < 2; ++h) {
         const uint64_t q = 2 * j + h;
         const int slot = (int)(q % HS);
-        if (!wait(&bar_full[slot], (uint32_t)((q / HS) & 1))) {
+        // K-half h of the A region is free once tile j-1's MMAs on it are done
+        if ((j >= 1 && !wait(&bar_a_free[h], (uint32_t)((j - 1) & 1))) ||
+            !wait(&bar_full[slot], (uint32_t)((q / HS) & 1))) {
           ok = false;
           break;
         }
+        tc_fence_after();
         const unsigned char* img = raw + slot * Cfg::HALF_BYTES;
 #pragma unroll
         for (int part = 0; part < K / 32; ++part) {
@@ -539,11 +544,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tmem_st16(areg + (uint32_t)(K + h * (K / 2) + part * 16), lo);
         }
         arrive(&bar_free[slot]);  // the direct epilogue never reads the image
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        tc_fence_before();
+        arrive(&bar_a_ready[h]);
       }
-      if (!ok) break;
-      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-      tc_fence_before();
-      arrive(&bar_a_ready[0]);
     }
   } else if (warp < 8) {
     // ----------------------------------------------------------- converters
@@ -565,21 +569,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if ((lane_row >> gb) & 1) gtile |= 8u << jb;
         ++gb;
       }
-    for (uint64_t j = 0; j < count; ++j) {
+    constexpr int KH = Cfg::SPLIT ? 2 : 1;  // K-halves handed over separately
+    bool ok = true;
+    for (uint64_t j = 0; j < count && ok; ++j) {
       const int slot = (int)(j % S);
       if (!wait(&bar_full[slot], (uint32_t)((j / S) & 1))) break;
       // the A region is free once the MMAs that read it last have completed:
-      // tile j-2's (two regions), or tile j-1's second pass (one region)
-      if constexpr (Cfg::SPLIT) {
-        if (j >= 1 && !wait(&bar_mma[1], (uint32_t)((j - 1) & 1))) break;
-      } else {
+      // tile j-2's (two regions); with one region (k = 6), each K-half once
+      // tile j-1's MMAs on that half are done
+      if constexpr (!Cfg::SPLIT) {
         if (j >= 2 && !wait(&bar_mma[j & 1], (uint32_t)(((j - 2) >> 1) & 1))) break;
       }
       tc_fence_after();
       const unsigned char* img = raw + slot * Cfg::RAW_BYTES;
       const uint32_t areg = tmem + lane_off + (uint32_t)((j % Cfg::A_BUFS) * Cfg::A_COLS);
+      for (int kh = 0; kh < KH; ++kh) {
+      if constexpr (Cfg::SPLIT) {
+        if (j >= 1 && !wait(&bar_a_free[kh], (uint32_t)((j - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+      }
 #pragma unroll
-      for (int part = 0; part < K / 16; ++part) {
+      for (int pp = 0; pp < K / 16 / KH; ++pp) {
+        const int part = kh * (K / 16 / KH) + pp;
         uint32_t hi[16], lo[16];
         uint32_t xs[16];
         if (g.tma_dims) {
@@ -614,7 +628,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
       asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       tc_fence_before();
-      arrive(&bar_a_ready[j % Cfg::A_BUFS]);
+      arrive(&bar_a_ready[Cfg::SPLIT ? kh : (int)(j % Cfg::A_BUFS)]);
+      }
+      if (!ok) break;
       if (g.direct) arrive(&bar_free[slot]);  // nothing else reads this image
     }
   } else if (warp < 12) {
@@ -715,7 +731,42 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     constexpr uint32_t idesc = tf32_idesc<Cfg::NH>();
     const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
     bool ok = true;
-    for (uint64_t j = 0; j < count && ok; ++j) {
+    if constexpr (Cfg::SPLIT) {
+      // k = 6, by K-half: both output halves over K-half 0 (then the
+      // converters may refill it), then both over K-half 1, each output half
+      // into its own accumulator; an accumulator is complete, and handed to
+      // the epilogue, after its K-half-1 MMAs
+      const uint32_t ah = tmem, al = tmem + (uint32_t)K;
+      for (uint64_t j = 0; j < count && ok; ++j) {
+        for (int kh = 0; kh < 2 && ok; ++kh) {
+          if (!wait(&bar_a_ready[kh], (uint32_t)(j & 1))) {
+            ok = false;
+            break;
+          }
+          for (int h = 0; h < 2; ++h) {
+            const uint64_t u = 2 * j + h;
+            if (kh == 0 && u >= 2 && !wait(&bar_acc_free[u & 1], (uint32_t)(((u >> 1) - 1) & 1))) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t acc = tmem + (uint32_t)(Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS);
+            const uint32_t hoff = (uint32_t)(h * Cfg::NH * 128);
+#pragma unroll
+            for (int sk = 0; sk < Cfg::KSTEPS / 2; ++sk) {
+              const int st = kh * (Cfg::KSTEPS / 2) + sk;
+              const uint32_t kbo = (uint32_t)((st >> 2) * N * 128 + (st & 3) * 32) + hoff;
+              tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
+              tc_mma_tf32_ts(acc + Cfg::NH, ah + 8 * st, sw128_desc(bl + kbo), idesc, st > 0 ? 1u : 0u);
+              tc_mma_tf32_ts(acc + Cfg::NH, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
+            }
+            if (kh == 1) tc_commit(smem_u32(&bar_mma[h]));
+          }
+          if (ok) tc_commit(smem_u32(&bar_a_free[kh]));
+        }
+      }
+    }
+    for (uint64_t j = 0; j < count && ok && !Cfg::SPLIT; ++j) {
       if (!wait(&bar_a_ready[j % Cfg::A_BUFS], (uint32_t)((j / Cfg::A_BUFS) & 1))) break;
       const uint32_t ah = tmem + (uint32_t)((j % Cfg::A_BUFS) * Cfg::A_COLS);
       const uint32_t al = ah + (uint32_t)K;
