@@ -513,6 +513,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     bool ok = true;
     for (uint64_t j = 0; j < count && ok; ++j) {
       const uint32_t areg = tmem + lane_off;
+#pragma unroll
       for (int h = 0; h < 2; ++h) {
         const uint64_t q = 2 * j + h;
         const int slot = (int)(q % HS);
@@ -583,6 +584,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tc_fence_after();
       const unsigned char* img = raw + slot * Cfg::RAW_BYTES;
       const uint32_t areg = tmem + lane_off + (uint32_t)((j % Cfg::A_BUFS) * Cfg::A_COLS);
+#pragma unroll
       for (int kh = 0; kh < KH; ++kh) {
       if constexpr (Cfg::SPLIT) {
         if (j >= 1 && !wait(&bar_a_free[kh], (uint32_t)((j - 1) & 1))) {
@@ -651,6 +653,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       bool ok = true;
       for (uint64_t j = 0; j < count && ok; ++j) {
         float2* dst = nullptr;
+#pragma unroll
         for (int h = 0; h < Cfg::PASSES; ++h) {
           const uint64_t u = j * Cfg::PASSES + h;  // accumulator use: region u%2, its (u/2)-th
           if (!wait(&bar_mma[u & 1], (uint32_t)((u >> 1) & 1))) {
@@ -686,6 +689,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     for (uint64_t j = 0; j < count && ok; ++j) {
       const int slot = (int)(j % S);
       unsigned char* out = raw + slot * Cfg::RAW_BYTES;
+#pragma unroll
       for (int h = 0; h < Cfg::PASSES; ++h) {
         const uint64_t u = j * Cfg::PASSES + h;
         if (!wait(&bar_mma[u & 1], (uint32_t)((u >> 1) & 1))) {
