@@ -68,8 +68,15 @@ struct TcCfg {
   static constexpr int NH = N / PASSES;  // accumulator columns of one MMA pass
   static constexpr int A_BUFS = SPLIT ? 1 : 2;
   static constexpr int A_COLS = 2 * K;
-  static constexpr int ACC_COLS = 2 * NH;
-  static constexpr int TMEM_COLS = A_BUFS * A_COLS + 2 * ACC_COLS;
+  // k <= 5: two accumulator regions (tile parity), each main | correction.
+  // k = 6: the three products of a pass go into one accumulator, so four
+  // regions fit (output half x tile parity) and the next tile's MMAs never
+  // wait for this tile's epilogue; the larger FP32 rounding drift of one
+  // accumulator is what the plan's norm restore corrects.
+  static constexpr bool CORR = !SPLIT;
+  static constexpr int ACC_REGIONS = SPLIT ? 4 : 2;
+  static constexpr int ACC_COLS = CORR ? 2 * NH : NH;
+  static constexpr int TMEM_COLS = A_BUFS * A_COLS + ACC_REGIONS * ACC_COLS;
   // staging images: as many as fit next to the B images (loads in flight)
   static constexpr int SLOTS_FIT = (kSmemBudget - 1024 - 2 * B_BYTES) / RAW_BYTES;
   static constexpr int SLOTS = SLOTS_FIT > 12 ? 12 : SLOTS_FIT;
@@ -278,7 +285,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   constexpr int SB = Cfg::SB;
   constexpr int HS = Cfg::HSLOTS > 0 ? Cfg::HSLOTS : 1;
   __shared__ __align__(8) uint64_t bar_full[SB], bar_free[SB];
-  __shared__ __align__(8) uint64_t bar_a_ready[2], bar_mma[2], bar_acc_free[2];
+  constexpr int AR = Cfg::ACC_REGIONS;
+  __shared__ __align__(8) uint64_t bar_a_ready[2], bar_mma[AR], bar_acc_free[AR];
   // k = 6: bar_a_ready[k] / bar_a_free[k] hand K-half k of the one A region
   // (A columns 64k..64k+63 and their lo copy) between converters and MMAs
   __shared__ __align__(8) uint64_t bar_a_free[2];
@@ -301,9 +309,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(smem_u32(&bar_a_ready[i]), kConverters);
+      mbar_init(smem_u32(&bar_a_free[i]), 1);
+    }
+    for (int i = 0; i < AR; ++i) {
       mbar_init(smem_u32(&bar_mma[i]), 1);
       mbar_init(smem_u32(&bar_acc_free[i]), kEpilogue);
-      mbar_init(smem_u32(&bar_a_free[i]), 1);
     }
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -656,7 +666,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
         for (int h = 0; h < Cfg::PASSES; ++h) {
           const uint64_t u = j * Cfg::PASSES + h;  // accumulator use: region u%2, its (u/2)-th
-          if (!wait(&bar_mma[u & 1], (uint32_t)((u >> 1) & 1))) {
+          if (!wait(&bar_mma[u % AR], (uint32_t)((u / AR) & 1))) {
             ok = false;
             break;
           }
@@ -664,13 +674,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           // tile j's base is in the ring once its MMAs are done (the
           // producer wrote it before the tile's copy was even issued)
           if (h == 0) dst = s + base_ring[j % R] + gdep;
-          const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS) +
+          const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u % AR) * Cfg::ACC_COLS) +
                                ((uint32_t)(32 * q) << 16);
 #pragma unroll
           for (int part = 0; part < Cfg::NH / 16; ++part) {
             float vm[16], vc[16];
             tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
-            tmem_ld<16>(acc + (uint32_t)(Cfg::NH + part * 16), vc);
+            if constexpr (Cfg::CORR) tmem_ld<16>(acc + (uint32_t)(Cfg::NH + part * 16), vc);
+            else
+#pragma unroll
+              for (int i = 0; i < 16; ++i) vc[i] = 0.f;
             tmem_ld_wait();
 #pragma unroll
             for (int i = 0; i < 8; ++i)
@@ -678,7 +691,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                   make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
           }
           tc_fence_before();
-          arrive(&bar_acc_free[u & 1]);
+          arrive(&bar_acc_free[u % AR]);
         }
       }
     } else {
@@ -692,18 +705,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
       for (int h = 0; h < Cfg::PASSES; ++h) {
         const uint64_t u = j * Cfg::PASSES + h;
-        if (!wait(&bar_mma[u & 1], (uint32_t)((u >> 1) & 1))) {
+        if (!wait(&bar_mma[u % AR], (uint32_t)((u / AR) & 1))) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS) +
+        const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u % AR) * Cfg::ACC_COLS) +
                              ((uint32_t)(32 * q) << 16);
 #pragma unroll
         for (int part = 0; part < Cfg::NH / 16; ++part) {
           float vm[16], vc[16];
           tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
-          tmem_ld<16>(acc + (uint32_t)(Cfg::NH + part * 16), vc);
+          if constexpr (Cfg::CORR) tmem_ld<16>(acc + (uint32_t)(Cfg::NH + part * 16), vc);
+          else
+#pragma unroll
+            for (int i = 0; i < 16; ++i) vc[i] = 0.f;
           tmem_ld_wait();
           if (q0_group) {
 #pragma unroll
@@ -719,7 +735,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           }
         }
         tc_fence_before();
-        arrive(&bar_acc_free[u & 1]);
+        arrive(&bar_acc_free[u % AR]);
       }
       if (!ok) break;
       asm volatile("bar.sync 1, %0;" ::"n"(kEpilogue) : "memory");
@@ -749,22 +765,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           }
           for (int h = 0; h < 2; ++h) {
             const uint64_t u = 2 * j + h;
-            if (kh == 0 && u >= 2 && !wait(&bar_acc_free[u & 1], (uint32_t)(((u >> 1) - 1) & 1))) {
+            if (kh == 0 && u >= (uint64_t)AR &&
+                !wait(&bar_acc_free[u % AR], (uint32_t)(((u / AR) - 1) & 1))) {
               ok = false;
               break;
             }
             tc_fence_after();
-            const uint32_t acc = tmem + (uint32_t)(Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS);
+            const uint32_t acc = tmem + (uint32_t)(Cfg::A_COLS + (u % AR) * Cfg::ACC_COLS);
             const uint32_t hoff = (uint32_t)(h * Cfg::NH * 128);
 #pragma unroll
             for (int sk = 0; sk < Cfg::KSTEPS / 2; ++sk) {
               const int st = kh * (Cfg::KSTEPS / 2) + sk;
               const uint32_t kbo = (uint32_t)((st >> 2) * N * 128 + (st & 3) * 32) + hoff;
               tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
-              tc_mma_tf32_ts(acc + Cfg::NH, ah + 8 * st, sw128_desc(bl + kbo), idesc, st > 0 ? 1u : 0u);
-              tc_mma_tf32_ts(acc + Cfg::NH, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
+              tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bl + kbo), idesc, 1u);
+              tc_mma_tf32_ts(acc, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
             }
-            if (kh == 1) tc_commit(smem_u32(&bar_mma[h]));
+            if (kh == 1) tc_commit(smem_u32(&bar_mma[u % AR]));
           }
           if (ok) tc_commit(smem_u32(&bar_a_free[kh]));
         }
