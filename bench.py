@@ -529,6 +529,22 @@ def main():
         checks["unfused_ms"] = min(un_ms)
         checks["speedup_vs_unfused"] = min(un_ms) / ms_step
         un_plan.close()
+        # the same circuit planned with 6-qubit blocks (fewer passes, each
+        # slower on the tensor cores): device time per circuit, best of 3
+        k6_plan = ket.Plan(nq, ops, ket.make_options("c64", args.fusion, 6, True))
+        k6_ms = []
+        for _ in range(3):
+            _lib.check(lib.ketgpu_state_reset(state.handle))
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            _lib.check(lib.ketgpu_plan_execute(k6_plan._h, state.handle))
+            a1.record(stream)
+            _lib.check(lib.ketgpu_state_synchronize(state.handle))
+            k6_ms.append(a0.elapsed_time(a1))
+        checks["k6_plan_ms"] = min(k6_ms)
+        checks["k6_plan_passes"] = int(k6_plan.stats()["n_passes"])
+        k6_plan.close()
 
     # dense-block kernel roofline (tensor-core passes)
     tc_idx = [i for i, x in enumerate(info) if x[0] == 2 and x[2] == 1]
