@@ -202,6 +202,9 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     ap.add_argument("--save", default=DEFAULT_MODEL)
     ap.add_argument("--nmax", type=int, default=32)
     ap.add_argument("--load", default=None, help="evaluate this trained model (skips measuring and training)")
+    ap.add_argument("--measure-budget-s", type=float, default=0.0,
+                    help="stop timing training circuits after this many seconds (0: no limit); the record "
+                         "states how many circuits were timed")
     args = ap.parse_args(argv)
 
     circs = corpus(args.train + args.eval, nmax=args.nmax)
@@ -213,7 +216,11 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     X, Y = [], []
     if args.load:
         train_spec = []
+    timed_circuits = 0
     for j, (n, d, s) in enumerate(train_spec):
+        if args.measure_budget_s > 0 and time.time() - t0 > args.measure_budget_s:
+            break
+        timed_circuits += 1
         c = random_mixed(n, d, seed=s)
         sub = c
         if args.train_gates > 0:
@@ -275,6 +282,10 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
         else:
             t_learned = float(timed_execute(p_learned, st_).sum())
             t_greedy = float(timed_execute(p_greedy, st_).sum())
+        # the best fixed alternative: greedy growth with 6-qubit blocks
+        p_greedy6 = Plan(n, c.to_ops(), make_options("c64", "greedy", 6, True))
+        t_greedy6 = float(timed_execute(p_greedy6, st_).sum())
+        p_greedy6.close()
         same = plan_signature(p_greedy) == plan_signature(p_learned)
         if not same:  # two more alternating timings of each plan, best of three
             st = _state(n)
@@ -283,7 +294,7 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
                 t_learned = min(t_learned, float(timed_execute(p_learned, st).sum()))
         pred_learned = float(p_learned.stats()["predicted_us"]) / 1e3
         row = {"n": n, "depth": d, "seed": s, "gates": int(p_greedy.stats()["n_gates"]),
-               "greedy_ms": t_greedy, "learned_ms": t_learned, "learned_pred_ms": pred_learned,
+               "greedy_ms": t_greedy, "learned_ms": t_learned, "greedy6_ms": t_greedy6, "learned_pred_ms": pred_learned,
                "greedy_passes": int(p_greedy.stats()["n_passes"]), "learned_passes": int(p_learned.stats()["n_passes"]),
                "same_plan": bool(same)}
         if i in unfused_set or i in check_set:
@@ -318,12 +329,15 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
     summary = {
         "model": model_path,
         "model_sha256": hashlib.sha256(open(model_path, "rb").read()).hexdigest(),
-        "train_circuits": len(train_spec), "train_gates_per_circuit": args.train_gates or "all",
+        "train_circuits": len(train_spec), "train_circuits_timed": timed_circuits if not args.load else 0,
+        "train_gates_per_circuit": args.train_gates or "all",
         "eval_circuits": len(eval_spec), "train_rows": int(len(X)),
         "measure_s": t_measure, "train_s": t_train, "loss_initial": loss0, "loss_final": loss,
         "loss_curve": curve, "train_rmse_log_us": train_rmse,
         "eval_total_greedy_ms": float(gt.sum()), "eval_total_learned_ms": float(lt.sum()),
         "eval_learned_over_greedy": float(lt.sum() / gt.sum()),
+        "eval_learned_over_greedy_k6": float(lt.sum() / sum(r["greedy6_ms"] for r in rows)),
+        "eval_greedy_k6_over_greedy": float(sum(r["greedy6_ms"] for r in rows) / gt.sum()),
         "eval_learned_over_greedy_geomean": float(np.exp(np.mean(np.log(lt / gt)))),
         "eval_same_plan_count": int(sum(r["same_plan"] for r in rows)),
         "eval_differing_plans": int(sum(not r["same_plan"] for r in rows)),
