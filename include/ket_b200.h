@@ -77,8 +77,9 @@ enum ketgpu_fusion {
 typedef struct ketgpu_options {
   int32_t precision;        /* ketgpu_precision */
   int32_t fusion;           /* ketgpu_fusion */
-  int32_t max_block_qubits; /* k <= 6 (fused blocks); 0 = default (5) */
-  int32_t tensor_cores;     /* 1: complex64 blocks on tcgen05 (3xTF32); 0: SIMT */
+  int32_t max_block_qubits; /* k <= 6 (fused blocks); 0 = default: 6 for
+                               complex64 with tensor_cores, else 5 */
+  int32_t tensor_cores;     /* 1: complex64 blocks on tcgen05 (3xFP16); 0: SIMT */
   int32_t renormalize;      /* 0: restore the starting norm after tensor-core
                                blocks (their FP32 accumulation rounds toward
                                zero); -1: never; 1: after every plan */

@@ -26,7 +26,7 @@ _PRECISIONS = {"c64": C64, "complex64": C64, "c128": C128, "complex128": C128}
 _FUSIONS = {"none": FUSE_NONE, "unfused": FUSE_NONE, "reference": FUSE_REFERENCE,
             "greedy": FUSE_GREEDY, "learned": FUSE_LEARNED}
 
-_opts = _lib.Options(C128, FUSE_GREEDY, 5, 1, 0)
+_opts = _lib.Options(C128, FUSE_GREEDY, 0, 1, 0)
 _num_threads = [1]
 
 
@@ -65,10 +65,11 @@ def get_options() -> dict:
             "max_block_qubits": _opts.max_block_qubits, "tensor_cores": bool(_opts.tensor_cores)}
 
 
-def make_options(precision="c128", fusion="greedy", max_block_qubits=5, tensor_cores=True,
+def make_options(precision="c128", fusion="greedy", max_block_qubits=0, tensor_cores=True,
                  renormalize=0) -> _lib.Options:
-    """renormalize: 0 restores the starting norm after tensor-core blocks,
-    -1 never, 1 after every plan."""
+    """max_block_qubits 0 takes the library default (6 for complex64 on the
+    tensor cores, else 5); renormalize: 0 restores the starting norm after
+    tensor-core blocks, -1 never, 1 after every plan."""
     return _lib.Options(_PRECISIONS[precision] if isinstance(precision, str) else int(precision),
                         _FUSIONS[fusion] if isinstance(fusion, str) else int(fusion),
                         int(max_block_qubits), 1 if tensor_cores else 0, int(renormalize))

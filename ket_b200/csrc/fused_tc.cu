@@ -5,32 +5,43 @@
 // the state is complex64.
 //
 // Formulation.  A tile is 128 groups x 2^k target combinations; group g's
-// amplitudes, interleaved (re, im), form row g of A (K = 2^(k+1) floats).
+// amplitudes, interleaved (re, im), form row g of A (K = 2^(k+1) reals).
 // With B the real embedding of the block matrix M,
 //     B[2c][2r] = Re M[r][c]   B[2c+1][2r] = -Im M[r][c]
 //     B[2c][2r+1] = Im M[r][c] B[2c+1][2r+1] = Re M[r][c],
 // the tile's output rows are D = A B, so the state is consumed in its own
-// interleaved layout.  Precision: 3xTF32 -- A and B are split into
-// hi = tf32(x) and lo = x - hi, and D = Ahi Bhi + Ahi Blo + Alo Bhi is
-// accumulated in FP32 in tensor memory (tcgen05.mma kind::tf32, M=128,
-// N=K=2^(k+1)).
+// interleaved layout.  Precision: 3xFP16 with power-of-two scaling.  Each A
+// row is scaled by 2^s (its largest magnitude into [2^14, 2^15)) and B by
+// 2^sb, both split into hi = fp16(x) and lo = fp16(x - hi) (11 significant
+// bits each, the split of 3xTF32), and D = Ahi Bhi + Ahi Blo + Alo Bhi is
+// accumulated in FP32 in tensor memory (tcgen05.mma kind::f16, M=128,
+// N=K=2^(k+1)) and scaled back by 2^-(s+sb) in the epilogue.  The scaling
+// keeps both halves in fp16's normal range whatever the amplitudes'
+// magnitude, so an element's error stays within 2^-22 of itself plus
+// 2^-39 of its row's largest; fp16 halves run the MMAs at twice the TF32
+// rate and take half the tensor and shared memory.
 //
 // Pipeline (one CTA per SM, persistent over tiles, warp-specialised):
 //   raw tiles into a ring of staging images -- one tiled tensor copy per
-//   tile when qubits 0..4 are group bits, per-thread cp.async otherwise ->
-//   converter warps split hi/lo into tensor memory -> one thread issues the
-//   MMAs, tcgen05.commit signals an mbarrier -> while tile j's MMAs run, the
-//   epilogue drains tile j-1's accumulator (double-buffered in TMEM) back to
-//   global memory, straight from registers or through shared memory.  Every
-//   mbarrier wait is bounded; on timeout the kernel raises an error flag,
-//   drains its copies, frees its tensor memory and returns.
+//   tile (two half-tile copies for k = 6) when qubits 0 and 1 are group
+//   bits, per-thread cp.async otherwise -> converter warps scale and split
+//   hi/lo into tensor memory (two A regions, tile parity) -> one thread
+//   issues the MMAs, tcgen05.commit signals an mbarrier -> while tile j's
+//   MMAs run, the epilogue drains tile j-1's accumulator (double-buffered in
+//   TMEM) back to global memory, straight from registers or through shared
+//   memory.  Every mbarrier wait is bounded; on timeout the kernel raises an
+//   error flag, drains its copies, frees its tensor memory and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "internal.h"
@@ -49,49 +60,36 @@ constexpr int kSmemBudget = 232448 - 1024;  // opt-in limit less static shared m
 template <int KQ>
 struct TcCfg {
   static constexpr int DIM = 1 << KQ;
-  static constexpr int K = 2 * DIM;           // floats per A row
+  static constexpr int K = 2 * DIM;           // reals per A row
   static constexpr int N = 2 * DIM;           // accumulator columns
   static constexpr int TB = KQ + kGroupBits;  // tile bits
   static constexpr int TILE = 1 << TB;        // amplitudes per tile
-  static constexpr int RAW_BYTES = TILE * 8;  // one staging image (= one A image)
-  static constexpr int B_BYTES = N * K * 4;   // one B image
-  static constexpr int KSTEPS = K / 8;        // tf32 MMA K = 8
-  // Tensor memory: A regions (hi | lo, 2K columns) and two accumulator
-  // regions (main | correction).  k <= 5: two A regions (tile parity) and one
-  // MMA pass of N columns per tile.  k = 6 (SPLIT): 2K + 2 * 2N would need
-  // 1024 columns, so one A region and two passes of N/2 columns per tile,
-  // each into its own accumulator region: the epilogue drains the first half
-  // while the second half's MMAs run, and the next tile's split waits only
-  // for this tile's MMAs.
-  static constexpr bool SPLIT = KQ == 6;
-  static constexpr int PASSES = SPLIT ? 2 : 1;
-  static constexpr int NH = N / PASSES;  // accumulator columns of one MMA pass
-  static constexpr int A_BUFS = SPLIT ? 1 : 2;
-  static constexpr int A_COLS = 2 * K;
-  // k <= 5: two accumulator regions (tile parity), each main | correction.
-  // k = 6: the three products of a pass go into one accumulator, so four
-  // regions fit (output half x tile parity) and the next tile's MMAs never
-  // wait for this tile's epilogue; the larger FP32 rounding drift of one
-  // accumulator is what the plan's norm restore corrects.
-  static constexpr bool CORR = !SPLIT;
-  static constexpr int ACC_REGIONS = SPLIT ? 4 : 2;
-  static constexpr int ACC_COLS = CORR ? 2 * NH : NH;
-  static constexpr int TMEM_COLS = A_BUFS * A_COLS + ACC_REGIONS * ACC_COLS;
+  static constexpr int RAW_BYTES = TILE * 8;  // one staging image (the FP32 tile)
+  // one fp16 B image: whole 128-byte swizzle atoms (64 halves) along K, so
+  // k = 4 (K = 32) leaves the upper half of each atom row unused
+  static constexpr int B_BYTES = (K + 63) / 64 * N * 128;
+  static constexpr int KSTEPS = K / 16;       // f16 MMA K = 16
+  // Tensor memory: two A regions (tile parity), each hi | lo with two fp16
+  // per 32-bit column (K columns), and two accumulator regions of N FP32
+  // columns; all three products of a tile go into one accumulator.
+  static constexpr int A_COLS = K;
+  static constexpr int TMEM_COLS = 2 * A_COLS + 2 * N;
   // staging images: as many as fit next to the B images (loads in flight)
   static constexpr int SLOTS_FIT = (kSmemBudget - 1024 - 2 * B_BYTES) / RAW_BYTES;
   static constexpr int SLOTS = SLOTS_FIT > 12 ? 12 : SLOTS_FIT;
   // k = 6 with a tensor copy: half-tile staging slots (the tile split by its
-  // highest target qubit), so copies run ahead of the split
+  // highest target qubit), so copies run further ahead of the converters
+  static constexpr bool HALVES = KQ == 6;
   static constexpr int HALF_BYTES = RAW_BYTES / 2;
-  static constexpr int HSLOTS = SPLIT ? (kSmemBudget - 1024 - 2 * B_BYTES) / HALF_BYTES : 0;
+  static constexpr int HSLOTS = HALVES ? (kSmemBudget - 1024 - 2 * B_BYTES) / HALF_BYTES : 0;
   static constexpr int SB = SLOTS > HSLOTS ? SLOTS : HSLOTS;  // barrier pairs
   static constexpr size_t STAGE = (size_t)SLOTS * RAW_BYTES > (size_t)HSLOTS * HALF_BYTES
                                       ? (size_t)SLOTS * RAW_BYTES
                                       : (size_t)HSLOTS * HALF_BYTES;
   static constexpr size_t SMEM = STAGE + 2 * B_BYTES + 1024;  // + alignment slack
   static_assert(TMEM_COLS <= 512 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory budget");
-  static_assert(SLOTS >= (SPLIT ? 1 : 3), "shared memory budget");
-  static_assert(!SPLIT || HSLOTS >= 3, "shared memory budget");
+  static_assert(SLOTS >= (HALVES ? 2 : 3), "shared memory budget");
+  static_assert(!HALVES || HSLOTS >= 4, "shared memory budget");
   static_assert(SMEM <= (size_t)kSmemBudget + 1024, "shared memory budget");
 };
 
@@ -104,7 +102,7 @@ struct TcGeom {
   int direct;         // the epilogue stores from registers (see launch_fused_tc)
   // Tensor-copy producer (tma_dims > 0, see launch_tc): dimension i of the
   // tensor map starts at qubit tma_start[i]; a tile's coordinate in it is
-  // (base >> tma_start[i]) & tma_mask[i].  ctile[c] = byte offset of
+  // (base >> tma_start[i]) & tma_mask[i].  ctile[c] = swizzled byte offset of
   // combination c in the tile image (natural tile index order).
   int tma_dims;
   int tma_start[5];
@@ -134,11 +132,20 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
-// Byte offset of element (row, kk) of a K-major SW128 image with `rows` rows.
+// Byte offset of FP32 element (row, kk) of a K-major SW128 image with `rows`
+// rows (the staging images).
 __host__ __device__ __forceinline__ uint32_t sw128_offset(int row, int kk, int rows) {
   const int kb = kk >> 5;             // 32 fp32 per 128-byte atom row
   const int chunk = (kk & 31) >> 2;   // 16-byte chunk in the row
   return (uint32_t)(kb * rows * 128 + row * 128 + ((chunk ^ (row & 7)) << 4) + ((kk & 3) << 2));
+}
+
+// Byte offset of fp16 element (row, kk) of a K-major SW128 image with `rows`
+// rows (the B images).
+__host__ __device__ __forceinline__ uint32_t sw128_offset_h(int row, int kk, int rows) {
+  const int kb = kk >> 6;             // 64 fp16 per 128-byte atom row
+  const int chunk = (kk & 63) >> 3;   // 16-byte chunk in the row
+  return (uint32_t)(kb * rows * 128 + row * 128 + ((chunk ^ (row & 7)) << 4) + ((kk & 7) << 1));
 }
 
 __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
@@ -203,25 +210,28 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-// A from tensor memory (lanes = rows, columns = K), B from shared memory.
-__device__ __forceinline__ void tc_mma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
-                                               uint32_t idesc, uint32_t accumulate) {
+// A from tensor memory (lanes = rows, two fp16 of K per 32-bit column), B
+// from shared memory, D in tensor memory (FP32).
+__device__ __forceinline__ void tc_mma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
+                                              uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
       "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 
-// 32 lanes x 16 columns of 32-bit values from the warp's registers.
+// 32 lanes x 16 columns of 32-bit values from the warp's registers.  No
+// memory clobber: the store reads registers only, and as volatile asm it
+// keeps its order against the tcgen05 waits and fences, so the compiler may
+// move shared-memory reads of the next columns ahead of it.
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
   asm volatile(
       "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
           taddr),
       "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
-      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
-      : "memory");
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]));
 }
 
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
@@ -247,36 +257,38 @@ __device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float* v) {
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// Instruction descriptor, kind::tf32: D=F32 [4,6), A=B=TF32 [7,10)/[10,13),
+// Instruction descriptor, kind::f16: D=F32 [4,6), A=B=F16 (0) [7,10)/[10,13),
 // both K-major, N>>3 at [17,23), M>>4 at [24,29).
 template <int N>
-__host__ __device__ constexpr uint32_t tf32_idesc() {
+__host__ __device__ constexpr uint32_t f16_idesc() {
   static_assert(N % 16 == 0 && N >= 16 && N <= 256, "M = 128 needs N a multiple of 16 in [16, 256]");
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
 // Roles (13 warps): 0-3 producers (cp.async into staging images; with a
-// tensor map, thread 0 alone issues one tiled copy per tile), 4-7
-// converters (hi/lo split into the A images), 8-11 epilogue (TMEM -> staging
-// -> HBM; warp w reads TMEM lanes 32*(w%4)..+31), 12 the MMA issuer.
-// mbarriers hand each tile from stage to stage, so loads of later tiles,
-// the split of tile j+1, the MMAs of tile j and the drain of tile j-1
-// proceed concurrently.
+// tensor map, thread 0 alone issues one tiled copy per tile or half tile),
+// 4-7 converters (scale and hi/lo split into the A regions), 8-11 epilogue
+// (TMEM -> HBM, from registers or through a staging image; warp w reads TMEM
+// lanes 32*(w%4)..+31), 12 the MMA issuer.  mbarriers hand each tile from
+// stage to stage, so loads of later tiles, the split of tile j+1, the MMAs of
+// tile j and the drain of tile j-1 proceed concurrently.
 constexpr int kProducers = 128, kConverters = 128, kEpilogue = 128;
+constexpr int kScaleRing = 4;  // row scales in flight (see the converters)
 
 template <int KQ>
 __global__ void __launch_bounds__(kTcThreads, 1)
     fused_tc_kernel(float2* __restrict__ s, TcGeom g, const uint32_t* __restrict__ bimg,
                     const __grid_constant__ CUtensorMap tmap) {
   using Cfg = TcCfg<KQ>;
-  constexpr int N = Cfg::N, TILE = Cfg::TILE;
+  constexpr int N = Cfg::N, TILE = Cfg::TILE, DIM = Cfg::DIM;
   constexpr int CPT = TILE / 2 / kProducers;  // 16-byte chunks per producer / epilogue thread
   constexpr int S = Cfg::SLOTS;
   constexpr int K = Cfg::K;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
-  // [B hi][B lo][staging image 0..S-1]; a staging image receives the raw
-  // tile in the A layout, is read once by the converters (which put hi and lo
-  // into tensor memory), and then carries the accumulator back out.
+  // [B hi][B lo][staging images]; a staging image receives the raw tile (in
+  // the A layout with cp.async, in natural tile order with a tensor copy), is
+  // read by the converters, and with staged stores then carries the
+  // accumulator back out.
   unsigned char* base_ptr = smem_dyn + ((1024 - (smem_u32(smem_dyn) & 1023)) & 1023);
   unsigned char* b_hi = base_ptr;
   unsigned char* b_lo = b_hi + Cfg::B_BYTES;
@@ -285,19 +297,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   constexpr int SB = Cfg::SB;
   constexpr int HS = Cfg::HSLOTS > 0 ? Cfg::HSLOTS : 1;
   __shared__ __align__(8) uint64_t bar_full[SB], bar_free[SB];
-  constexpr int AR = Cfg::ACC_REGIONS;
-  __shared__ __align__(8) uint64_t bar_a_ready[2], bar_mma[AR], bar_acc_free[AR];
-  // k = 6: bar_a_ready[k] / bar_a_free[k] hand K-half k of the one A region
-  // (A columns 64k..64k+63 and their lo copy) between converters and MMAs
-  __shared__ __align__(8) uint64_t bar_a_free[2];
+  __shared__ __align__(8) uint64_t bar_a_ready[2], bar_mma[2], bar_acc_free[2], bar_scale[kScaleRing];
   __shared__ uint32_t tmem_base_slot;
   // Tile bases, written by the producer when it issues a tile and read by
-  // the epilogue once the tile's MMAs are done.  The producer can run at
-  // most 2S tiles ahead of the direct epilogue (k <= 5: it waits for a slot
-  // that the converters free only after MMAs that wait for the epilogue of
-  // four tiles back), and 3 with one slot (k = 6); R entries cover both.
+  // the epilogue once the tile's MMAs are done.  The producer runs at most
+  // S + 4 tiles (k = 6 in halves: 6) ahead of the epilogue: it waits for a
+  // slot that the converters free only after MMAs that wait for the
+  // epilogue of two tiles back.  R entries cover that.
   constexpr int R = 2 * S > 8 ? 2 * S : 8;
   __shared__ uint64_t base_ring[R];
+  // Per tile and TMEM lane: s + sb, the exponent the epilogue scales by.
+  __shared__ int8_t row_exp[kScaleRing][128];
   __shared__ volatile int abort_flag;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -305,16 +315,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (tid == 0) {
     for (int i = 0; i < SB; ++i) {
       mbar_init(smem_u32(&bar_full[i]), g.tma_dims ? 1 : kProducers + 1);
-      mbar_init(smem_u32(&bar_free[i]), kEpilogue);
+      mbar_init(smem_u32(&bar_free[i]), g.direct ? kConverters : kEpilogue);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(smem_u32(&bar_a_ready[i]), kConverters);
-      mbar_init(smem_u32(&bar_a_free[i]), 1);
-    }
-    for (int i = 0; i < AR; ++i) {
       mbar_init(smem_u32(&bar_mma[i]), 1);
       mbar_init(smem_u32(&bar_acc_free[i]), kEpilogue);
     }
+    for (int i = 0; i < kScaleRing; ++i) mbar_init(smem_u32(&bar_scale[i]), kConverters);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -363,6 +371,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   auto arrive = [](uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
   };
+  // Bounded drain of a copy's completion (no abort: the copy lands anyway).
+  auto drain = [](uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+      uint32_t done;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(done)
+          : "r"(a), "r"(parity)
+          : "memory");
+      if (done) return;
+    }
+  };
 
   // Chunk offsets shared by producers and epilogue threads: chunk
   // ch = t + 128*i covers tile amplitudes e = 2ch, 2ch+1 (address order, bit j
@@ -377,7 +400,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   // (r mod 64) * DIM + (c ^ (r mod 8)), so the store phase reads one 16-byte
   // word per chunk and the TMEM drain writes stay spread over the banks.
   auto pair_slot = [](int row, int comb) -> uint32_t {
-    return (uint32_t)(((row & 63) * Cfg::DIM + (comb ^ (row & 7))) * 16 + 8 * (row >> 6));
+    return (uint32_t)(((row & 63) * DIM + (comb ^ (row & 7))) * 16 + 8 * (row >> 6));
   };
   auto chunk_offsets = [&](int t, uint64_t* goff, uint32_t* soff, bool out_layout) {
 #pragma unroll
@@ -405,81 +428,37 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     return b;
   };
 
-  if (Cfg::SPLIT && warp < 4 && g.half) {
-    // ------------------------------- producer, k = 6 tensor copy in halves
-    // Half q = 2j + h of tile j (h: the highest target's bit) goes to slot
-    // q % HS; three slots let the copies run a tile and a half ahead.
-    if (tid == 0) {
-      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap)) : "memory");
-      uint64_t issued = 0;
-      for (uint64_t q = 0; q < 2 * count; ++q) {
-        const uint64_t j = q >> 1;
-        const int slot = (int)(q % HS);
-        if (q >= (uint64_t)HS && !wait(&bar_free[slot], (uint32_t)(((q / HS) - 1) & 1))) break;
-        uint64_t base = tile_base(first + j * stride);
-        if ((q & 1) == 0) base_ring[j % R] = base;
-        else base |= g.top_off;
-        const uint32_t bar = smem_u32(&bar_full[slot]);
-        mbar_arrive_expect_tx(bar, (uint32_t)Cfg::HALF_BYTES);
-        int crd[5];
-#pragma unroll
-        for (int i = 0; i < 5; ++i) crd[i] = (int)((base >> g.tma_start[i]) & g.tma_mask[i]);
-        tma_load_box(smem_u32(raw + slot * Cfg::HALF_BYTES), &tmap, crd, g.tma_dims, bar);
-        issued = q + 1;
-      }
-      // drain: every issued copy lands before the CTA may leave
-      for (uint64_t q = issued > (uint64_t)HS ? issued - HS : 0; q < issued; ++q) {
-        const uint32_t a = smem_u32(&bar_full[q % HS]);
-        for (uint32_t it = 0; it < kWaitLimit; ++it) {
-          uint32_t done;
-          asm volatile(
-              "{\n\t.reg .pred p;\n\t"
-              "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-              "selp.u32 %0, 1, 0, p;\n\t}"
-              : "=r"(done)
-              : "r"(a), "r"((uint32_t)((q / HS) & 1))
-              : "memory");
-          if (done) break;
-        }
-      }
-    }
-  } else if (warp < 4 && g.tma_dims) {
+  if (warp < 4 && g.tma_dims) {
     // ------------------------------------------ producer, tensor-copy form
-    // One thread fetches each whole tile with a single tiled tensor copy;
-    // the image holds the tile in its natural index order under the
+    // One thread fetches each tile with one tiled tensor copy (k = 6: two,
+    // half q = 2j + h of tile j -- h the highest target's bit -- into slot
+    // q % HS); an image holds its box in natural index order under the
     // 128-byte swizzle.
     if (tid == 0) {
       asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap)) : "memory");
+      constexpr int PER = Cfg::HALVES ? 2 : 1;  // copies per tile
+      constexpr int NS = Cfg::HALVES ? HS : S;
+      constexpr uint32_t BYTES = Cfg::HALVES ? Cfg::HALF_BYTES : Cfg::RAW_BYTES;
       uint64_t issued = 0;
-      for (uint64_t j = 0; j < count; ++j) {
-        const int slot = (int)(j % S);
-        if (j >= (uint64_t)S && !wait(&bar_free[slot], (uint32_t)(((j / S) - 1) & 1))) break;
-        const uint64_t base = tile_base(first + j * stride);
-        base_ring[j % R] = base;
+      for (uint64_t q = 0; q < PER * count; ++q) {
+        const uint64_t j = q / PER;
+        const int slot = (int)(q % NS);
+        if (q >= (uint64_t)NS && !wait(&bar_free[slot], (uint32_t)(((q / NS) - 1) & 1))) break;
+        uint64_t base = tile_base(first + j * stride);
+        if (q % PER == 0) base_ring[j % R] = base;
+        else base |= g.top_off;
         const uint32_t bar = smem_u32(&bar_full[slot]);
-        mbar_arrive_expect_tx(bar, (uint32_t)Cfg::RAW_BYTES);
+        mbar_arrive_expect_tx(bar, BYTES);
         int crd[5];
 #pragma unroll
         for (int i = 0; i < 5; ++i) crd[i] = (int)((base >> g.tma_start[i]) & g.tma_mask[i]);
-        tma_load_box(smem_u32(raw + slot * Cfg::RAW_BYTES), &tmap, crd, g.tma_dims, bar);
-        issued = j + 1;
+        tma_load_box(smem_u32(raw + slot * BYTES), &tmap, crd, g.tma_dims, bar);
+        issued = q + 1;
       }
-      // Drain: every issued tile's copy lands before the CTA may leave (on
-      // the normal path the converters have already seen them all).
-      for (uint64_t j = issued > (uint64_t)S ? issued - S : 0; j < issued; ++j) {
-        const uint32_t a = smem_u32(&bar_full[j % S]);
-        for (uint32_t it = 0; it < kWaitLimit; ++it) {
-          uint32_t done;
-          asm volatile(
-              "{\n\t.reg .pred p;\n\t"
-              "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-              "selp.u32 %0, 1, 0, p;\n\t}"
-              : "=r"(done)
-              : "r"(a), "r"((uint32_t)((j / S) & 1))
-              : "memory");
-          if (done) break;
-        }
-      }
+      // Drain: every issued copy lands before the CTA may leave (on the
+      // normal path the converters have already seen them all).
+      for (uint64_t q = issued > (uint64_t)NS ? issued - NS : 0; q < issued; ++q)
+        drain(&bar_full[q % NS], (uint32_t)((q / NS) & 1));
     }
   } else if (warp < 4) {
     // ------------------------------------------------------------ producers
@@ -509,147 +488,143 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
-  } else if (Cfg::SPLIT && warp < 8 && g.half) {
-    // --------------------------------- converters, k = 6 tensor copy in halves
-    // As below, with the row read from two half boxes: half h holds the
-    // combinations whose highest target bit is h, i.e. A columns 64h..64h+63.
-    const int q4 = warp & 3;
-    const int lane_row = 32 * q4 + lane;
-    const uint32_t lane_off = (uint32_t)(32 * q4) << 16;
-    uint32_t gtile = 0;
-#pragma unroll
-    for (int b = 0; b < kGroupBits; ++b)
-      if ((lane_row >> b) & 1) gtile |= g.gbit_off[b];
-    bool ok = true;
-    for (uint64_t j = 0; j < count && ok; ++j) {
-      const uint32_t areg = tmem + lane_off;
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const uint64_t q = 2 * j + h;
-        const int slot = (int)(q % HS);
-        // K-half h of the A region is free once tile j-1's MMAs on it are done
-        if ((j >= 1 && !wait(&bar_a_free[h], (uint32_t)((j - 1) & 1))) ||
-            !wait(&bar_full[slot], (uint32_t)((q / HS) & 1))) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const unsigned char* img = raw + slot * Cfg::HALF_BYTES;
-#pragma unroll
-        for (int part = 0; part < K / 32; ++part) {
-          uint32_t hi[16], lo[16], xs[16];
-#pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const uint32_t off = g.ctile[part * 8 + i] | gtile;
-            const uint2 x = *reinterpret_cast<const uint2*>(img + (off ^ ((off >> 3) & 0x70u)));
-            xs[2 * i] = x.x;
-            xs[2 * i + 1] = x.y;
-          }
-#pragma unroll
-          for (int u = 0; u < 16; ++u) {
-            const uint32_t hh = (xs[u] + 0x1000u) & 0xffffe000u;
-            hi[u] = hh;
-            lo[u] = (__float_as_uint(__uint_as_float(xs[u]) - __uint_as_float(hh)) + 0x1000u) & 0xffffe000u;
-          }
-          tmem_st16(areg + (uint32_t)(h * (K / 2) + part * 16), hi);
-          tmem_st16(areg + (uint32_t)(K + h * (K / 2) + part * 16), lo);
-        }
-        arrive(&bar_free[slot]);  // the direct epilogue never reads the image
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-        tc_fence_before();
-        arrive(&bar_a_ready[h]);
-      }
-    }
   } else if (warp < 8) {
     // ----------------------------------------------------------- converters
-    // Thread = A row (TMEM lane 32*(warp%4) + lane): read the row from the
-    // staging image, split x = hi + lo with hi = tf32(x) (round to nearest,
-    // ties away: magnitude bits plus half an ulp, truncated) and
-    // lo = tf32(x - hi), and store both into the A region of tile parity j%2
-    // in tensor memory once the MMAs of tile j-2 have released it.
-    // In the direct-store mode TMEM lane t carries group t (its staging row
-    // is the rotated one); otherwise lane t carries staging row t.
+    // Thread = A row (TMEM lane 32*(warp%4) + lane).  Per tile: the row's
+    // largest magnitude m sets s (m * 2^s in [2^14, 2^15)); each element
+    // x * 2^s splits into hi = fp16(x * 2^s), lo = fp16(x * 2^s - hi), two
+    // fp16 per 32-bit column (re low, im high), into the A region of tile
+    // parity j%2 once the MMAs of tile j-2 have released it; s + sb goes to
+    // the epilogue through row_exp.
+    // In the direct-store mode TMEM lane t carries group t (its cp.async
+    // staging row is the rotated one); otherwise lane t carries staging row t.
     const int q = warp & 3;
     const int lane_row = 32 * q + lane;
     const int row = g.direct ? ((lane_row >> 1) | ((lane_row & 1) << (kGroupBits - 1))) : lane_row;
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
-    // tensor-copy images: byte offset of this lane's group in the tile
+    const int sb = (int)bimg[2 * Cfg::B_BYTES / 4];
+    // tensor-copy images: byte offset of this lane's group in the tile (or
+    // in a half tile)
     uint32_t gtile = 0;
-    for (int jb = 0, gb = 0; jb < Cfg::TB; ++jb)
-      if (!g.is_target[jb]) {
-        if ((lane_row >> gb) & 1) gtile |= 8u << jb;
-        ++gb;
-      }
-    constexpr int KH = Cfg::SPLIT ? 2 : 1;  // K-halves handed over separately
-    bool ok = true;
-    for (uint64_t j = 0; j < count && ok; ++j) {
-      const int slot = (int)(j % S);
-      if (!wait(&bar_full[slot], (uint32_t)((j / S) & 1))) break;
-      // the A region is free once the MMAs that read it last have completed:
-      // tile j-2's (two regions); with one region (k = 6), each K-half once
-      // tile j-1's MMAs on that half are done
-      if constexpr (!Cfg::SPLIT) {
-        if (j >= 2 && !wait(&bar_mma[j & 1], (uint32_t)(((j - 2) >> 1) & 1))) break;
-      }
-      tc_fence_after();
-      const unsigned char* img = raw + slot * Cfg::RAW_BYTES;
-      const uint32_t areg = tmem + lane_off + (uint32_t)((j % Cfg::A_BUFS) * Cfg::A_COLS);
+    if (Cfg::HALVES && g.tma_dims) {
 #pragma unroll
-      for (int kh = 0; kh < KH; ++kh) {
-      if constexpr (Cfg::SPLIT) {
-        if (j >= 1 && !wait(&bar_a_free[kh], (uint32_t)((j - 1) & 1))) {
-          ok = false;
-          break;
+      for (int b = 0; b < kGroupBits; ++b)
+        if ((lane_row >> b) & 1) gtile |= g.gbit_off[b];
+    } else {
+      for (int jb = 0, gb = 0; jb < Cfg::TB; ++jb)
+        if (!g.is_target[jb]) {
+          if ((lane_row >> gb) & 1) gtile |= 8u << jb;
+          ++gb;
         }
+    }
+    // The 128-byte swizzle (16-byte chunk c of 128-byte row r at c ^ (r mod
+    // 8)) is linear over XOR, and group and target bits are disjoint, so an
+    // amplitude's swizzled offset is the swizzled group offset XOR the
+    // swizzled combination offset (ctile holds the latter).
+    const uint32_t gsw = gtile ^ ((gtile >> 3) & 0x70u);
+    // One loop per producer form, chosen once: with the form a compile-time
+    // constant, every staging read of a tile has a constant offset and the
+    // reads issue back to back (a per-read branch on the form kept only two
+    // in flight, each paying the full shared-memory latency).
+    auto convert_tiles = [&](auto form) {
+      constexpr bool TMA = decltype(form)::value;
+      constexpr bool HALF = TMA && Cfg::HALVES;
+      for (uint64_t j = 0; j < count; ++j) {
+        // the tile's images: one, or (k = 6 tensor copy) its two halves
+        int slot0, slot1;
+        bool ok;
+        if constexpr (HALF) {
+          slot0 = (int)((2 * j) % HS);
+          slot1 = (int)((2 * j + 1) % HS);
+          ok = wait(&bar_full[slot0], (uint32_t)(((2 * j) / HS) & 1)) &&
+               wait(&bar_full[slot1], (uint32_t)(((2 * j + 1) / HS) & 1));
+        } else {
+          slot0 = slot1 = (int)(j % S);
+          ok = wait(&bar_full[slot0], (uint32_t)((j / S) & 1));
+        }
+        // the A region is free once tile j-2's MMAs have completed
+        if (!ok || (j >= 2 && !wait(&bar_mma[j & 1], (uint32_t)(((j - 2) >> 1) & 1)))) break;
         tc_fence_after();
-      }
+        const unsigned char* img0 = raw + (HALF ? slot0 * Cfg::HALF_BYTES : slot0 * Cfg::RAW_BYTES);
+        const unsigned char* img1 = raw + slot1 * Cfg::HALF_BYTES;
+        // amplitudes 2i and 2i+1 of this row as (re, im, re, im)
+        auto amp_pair = [&](int i) -> float4 {
+          if constexpr (!TMA) {
+            return *reinterpret_cast<const float4*>(img0 + sw128_offset(row, 4 * i, 128));
+          } else {
+            float2 v[2];
 #pragma unroll
-      for (int pp = 0; pp < K / 16 / KH; ++pp) {
-        const int part = kh * (K / 16 / KH) + pp;
-        uint32_t hi[16], lo[16];
-        uint32_t xs[16];
-        if (g.tma_dims) {
-          // natural tile order under the 128-byte swizzle (16-byte chunk
-          // c of 128-byte row r sits at chunk c ^ (r mod 8)), which spreads
-          // lanes whose groups lie 128 B apart or more over the banks
+            for (int h = 0; h < 2; ++h) {
+              const int c = 2 * i + h;
+              const unsigned char* img = (HALF && c >= 32) ? img1 : img0;
+              v[h] = *reinterpret_cast<const float2*>(img + (g.ctile[HALF ? (c & 31) : c] ^ gsw));
+            }
+            return make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+          }
+        };
+        // the row's largest magnitude, eight amplitude pairs per batch
+        float m = 0.f;
+#pragma unroll
+        for (int bt = 0; bt < DIM / 16; ++bt) {
+          float4 v[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) v[i] = amp_pair(8 * bt + i);
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            m = fmaxf(m, fmaxf(fmaxf(fabsf(v[i].x), fabsf(v[i].y)), fmaxf(fabsf(v[i].z), fabsf(v[i].w))));
+        }
+        // m in [2^e, 2^(e+1)) has exponent field e + 127; s = 14 - e, kept
+        // within +-100 (a zero or subnormal row takes 100)
+        const int ef = (int)(__float_as_uint(m) >> 23);
+        const int sa = ef == 0 ? 100 : max(-100, min(100, 141 - ef));
+        row_exp[j % kScaleRing][lane_row] = (int8_t)(sa + sb);
+        arrive(&bar_scale[j % kScaleRing]);
+        const float sc = __int_as_float((127 + sa) << 23);
+        const uint32_t areg = tmem + lane_off + (uint32_t)((j & 1) * Cfg::A_COLS);
+#pragma unroll
+        for (int part = 0; part < K / 32; ++part) {
+          uint32_t hi[16], lo[16];
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            const uint32_t off = g.ctile[part * 8 + i] | gtile;
-            const uint2 x = *reinterpret_cast<const uint2*>(img + (off ^ ((off >> 3) & 0x70u)));
-            xs[2 * i] = x.x;
-            xs[2 * i + 1] = x.y;
-          }
-        } else {
+            const float4 v = amp_pair(8 * part + i);
+            const float xs[4] = {v.x * sc, v.y * sc, v.z * sc, v.w * sc};
 #pragma unroll
-          for (int c4 = 0; c4 < 4; ++c4) {
-            const uint4 x = *reinterpret_cast<const uint4*>(img + sw128_offset(row, part * 16 + 4 * c4, 128));
-            xs[4 * c4] = x.x;
-            xs[4 * c4 + 1] = x.y;
-            xs[4 * c4 + 2] = x.z;
-            xs[4 * c4 + 3] = x.w;
+            for (int u = 0; u < 2; ++u) {
+              const __half2 h = __floats2half2_rn(xs[2 * u], xs[2 * u + 1]);
+              const float2 hf = __half22float2(h);
+              const __half2 l = __floats2half2_rn(xs[2 * u] - hf.x, xs[2 * u + 1] - hf.y);
+              hi[2 * i + u] = *reinterpret_cast<const uint32_t*>(&h);
+              lo[2 * i + u] = *reinterpret_cast<const uint32_t*>(&l);
+            }
           }
+          tmem_st16(areg + (uint32_t)(part * 16), hi);
+          tmem_st16(areg + (uint32_t)(K / 2 + part * 16), lo);
         }
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const uint32_t h = (xs[u] + 0x1000u) & 0xffffe000u;
-          hi[u] = h;
-          lo[u] = (__float_as_uint(__uint_as_float(xs[u]) - __uint_as_float(h)) + 0x1000u) & 0xffffe000u;
+        if (g.direct) {  // nothing else reads the images
+          arrive(&bar_free[slot0]);
+          if (slot1 != slot0) arrive(&bar_free[slot1]);
         }
-        tmem_st16(areg + (uint32_t)(part * 16), hi);
-        tmem_st16(areg + (uint32_t)(K + part * 16), lo);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        tc_fence_before();
+        arrive(&bar_a_ready[j & 1]);
       }
-      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-      tc_fence_before();
-      arrive(&bar_a_ready[Cfg::SPLIT ? kh : (int)(j % Cfg::A_BUFS)]);
-      }
-      if (!ok) break;
-      if (g.direct) arrive(&bar_free[slot]);  // nothing else reads this image
-    }
+    };
+    if (g.tma_dims) convert_tiles(std::true_type{});
+    else convert_tiles(std::false_type{});
   } else if (warp < 12) {
     // ------------------------------------------------------------- epilogue
     const int t = tid - 256;
     const int q = warp & 3;
     const int row = 32 * q + lane;
+    const uint32_t acc_lane = tmem + (uint32_t)(2 * Cfg::A_COLS) + ((uint32_t)(32 * q) << 16);
+    // Waits for tile j's accumulator and row scale; returns 2^-(s + sb).
+    auto tile_ready = [&](uint64_t j, float* unscale) -> bool {
+      if (!wait(&bar_mma[j & 1], (uint32_t)((j >> 1) & 1))) return false;
+      tc_fence_after();
+      if (!wait(&bar_scale[j % kScaleRing], (uint32_t)((j / kScaleRing) & 1))) return false;
+      *unscale = __int_as_float((127 - (int)row_exp[j % kScaleRing][row]) << 23);
+      return true;
+    };
     if (g.direct) {
       // TMEM lane = group `row`; the lanes of a warp vary the five lowest
       // group bits, which include qubits 0 and 1, so each run of lanes
@@ -660,159 +635,82 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           if ((row >> gb) & 1) gdep |= uint64_t{1} << g.tile_pos[jb];
           ++gb;
         }
-      bool ok = true;
-      for (uint64_t j = 0; j < count && ok; ++j) {
-        float2* dst = nullptr;
+      for (uint64_t j = 0; j < count; ++j) {
+        float us;
+        if (!tile_ready(j, &us)) break;
+        // tile j's base is in the ring once its MMAs are done (the
+        // producer wrote it before the tile's copy was even issued)
+        float2* dst = s + base_ring[j % R] + gdep;
+        const uint32_t acc = acc_lane + (uint32_t)((j & 1) * N);
 #pragma unroll
-        for (int h = 0; h < Cfg::PASSES; ++h) {
-          const uint64_t u = j * Cfg::PASSES + h;  // accumulator use: region u%2, its (u/2)-th
-          if (!wait(&bar_mma[u % AR], (uint32_t)((u / AR) & 1))) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          // tile j's base is in the ring once its MMAs are done (the
-          // producer wrote it before the tile's copy was even issued)
-          if (h == 0) dst = s + base_ring[j % R] + gdep;
-          const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u % AR) * Cfg::ACC_COLS) +
-                               ((uint32_t)(32 * q) << 16);
+        for (int part = 0; part < N / 16; ++part) {
+          float v[16];
+          tmem_ld<16>(acc + (uint32_t)(part * 16), v);
+          tmem_ld_wait();
 #pragma unroll
-          for (int part = 0; part < Cfg::NH / 16; ++part) {
-            float vm[16], vc[16];
-            tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
-            if constexpr (Cfg::CORR) tmem_ld<16>(acc + (uint32_t)(Cfg::NH + part * 16), vc);
-            else
-#pragma unroll
-              for (int i = 0; i < 16; ++i) vc[i] = 0.f;
-            tmem_ld_wait();
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-              dst[g.cdep[h * (Cfg::NH / 2) + part * 8 + i]] =
-                  make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
-          }
-          tc_fence_before();
-          arrive(&bar_acc_free[u % AR]);
+          for (int i = 0; i < 8; ++i) dst[g.cdep[part * 8 + i]] = make_float2(v[2 * i] * us, v[2 * i + 1] * us);
         }
+        tc_fence_before();
+        arrive(&bar_acc_free[j & 1]);
       }
     } else {
-    uint64_t goff[CPT];
-    uint32_t soff[CPT];
-    chunk_offsets(t, goff, soff, true);
-    bool ok = true;
-    for (uint64_t j = 0; j < count && ok; ++j) {
-      const int slot = (int)(j % S);
-      unsigned char* out = raw + slot * Cfg::RAW_BYTES;
+      uint64_t goff[CPT];
+      uint32_t soff[CPT];
+      chunk_offsets(t, goff, soff, true);
+      for (uint64_t j = 0; j < count; ++j) {
+        const int slot = (int)(j % S);
+        unsigned char* out = raw + slot * Cfg::RAW_BYTES;
+        float us;
+        if (!tile_ready(j, &us)) break;
+        const uint32_t acc = acc_lane + (uint32_t)((j & 1) * N);
 #pragma unroll
-      for (int h = 0; h < Cfg::PASSES; ++h) {
-        const uint64_t u = j * Cfg::PASSES + h;
-        if (!wait(&bar_mma[u % AR], (uint32_t)((u / AR) & 1))) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u % AR) * Cfg::ACC_COLS) +
-                             ((uint32_t)(32 * q) << 16);
-#pragma unroll
-        for (int part = 0; part < Cfg::NH / 16; ++part) {
-          float vm[16], vc[16];
-          tmem_ld<16>(acc + (uint32_t)(part * 16), vm);
-          if constexpr (Cfg::CORR) tmem_ld<16>(acc + (uint32_t)(Cfg::NH + part * 16), vc);
-          else
-#pragma unroll
-            for (int i = 0; i < 16; ++i) vc[i] = 0.f;
+        for (int part = 0; part < N / 16; ++part) {
+          float v[16];
+          tmem_ld<16>(acc + (uint32_t)(part * 16), v);
           tmem_ld_wait();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) v[i] *= us;
           if (q0_group) {
 #pragma unroll
             for (int i = 0; i < 8; ++i)
-              *reinterpret_cast<float2*>(out + pair_slot(row, h * (Cfg::NH / 2) + part * 8 + i)) =
-                  make_float2(vm[2 * i] + vc[2 * i], vm[2 * i + 1] + vc[2 * i + 1]);
+              *reinterpret_cast<float2*>(out + pair_slot(row, part * 8 + i)) = make_float2(v[2 * i], v[2 * i + 1]);
           } else {
 #pragma unroll
             for (int i = 0; i < 4; ++i)
-              *reinterpret_cast<float4*>(out + sw128_offset(row, h * Cfg::NH + part * 16 + 4 * i, 128)) =
-                  make_float4(vm[4 * i] + vc[4 * i], vm[4 * i + 1] + vc[4 * i + 1], vm[4 * i + 2] + vc[4 * i + 2],
-                              vm[4 * i + 3] + vc[4 * i + 3]);
+              *reinterpret_cast<float4*>(out + sw128_offset(row, part * 16 + 4 * i, 128)) =
+                  make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
           }
         }
         tc_fence_before();
-        arrive(&bar_acc_free[u % AR]);
-      }
-      if (!ok) break;
-      asm volatile("bar.sync 1, %0;" ::"n"(kEpilogue) : "memory");
-      float2* dst = s + base_ring[j % R];
+        arrive(&bar_acc_free[j & 1]);
+        asm volatile("bar.sync 1, %0;" ::"n"(kEpilogue) : "memory");
+        float2* dst = s + base_ring[j % R];
 #pragma unroll
-      for (int i = 0; i < CPT; ++i)
-        *reinterpret_cast<float4*>(dst + goff[i]) = *reinterpret_cast<const float4*>(out + soff[i]);
-      arrive(&bar_free[slot]);
-    }
+        for (int i = 0; i < CPT; ++i)
+          *reinterpret_cast<float4*>(dst + goff[i]) = *reinterpret_cast<const float4*>(out + soff[i]);
+        arrive(&bar_free[slot]);
+      }
     }
   } else if (warp == 12 && lane == 0) {
     // ------------------------------------------------------------ MMA issue
-    constexpr uint32_t idesc = tf32_idesc<Cfg::NH>();
+    constexpr uint32_t idesc = f16_idesc<N>();
     const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
-    bool ok = true;
-    if constexpr (Cfg::SPLIT) {
-      // k = 6, by K-half: both output halves over K-half 0 (then the
-      // converters may refill it), then both over K-half 1, each output half
-      // into its own accumulator; an accumulator is complete, and handed to
-      // the epilogue, after its K-half-1 MMAs
-      const uint32_t ah = tmem, al = tmem + (uint32_t)K;
-      for (uint64_t j = 0; j < count && ok; ++j) {
-        for (int kh = 0; kh < 2 && ok; ++kh) {
-          if (!wait(&bar_a_ready[kh], (uint32_t)(j & 1))) {
-            ok = false;
-            break;
-          }
-          for (int h = 0; h < 2; ++h) {
-            const uint64_t u = 2 * j + h;
-            if (kh == 0 && u >= (uint64_t)AR &&
-                !wait(&bar_acc_free[u % AR], (uint32_t)(((u / AR) - 1) & 1))) {
-              ok = false;
-              break;
-            }
-            tc_fence_after();
-            const uint32_t acc = tmem + (uint32_t)(Cfg::A_COLS + (u % AR) * Cfg::ACC_COLS);
-            const uint32_t hoff = (uint32_t)(h * Cfg::NH * 128);
+    for (uint64_t j = 0; j < count; ++j) {
+      if (!wait(&bar_a_ready[j & 1], (uint32_t)((j >> 1) & 1))) break;
+      if (j >= 2 && !wait(&bar_acc_free[j & 1], (uint32_t)(((j >> 1) - 1) & 1))) break;
+      tc_fence_after();
+      const uint32_t ah = tmem + (uint32_t)((j & 1) * Cfg::A_COLS);
+      const uint32_t al = ah + (uint32_t)(K / 2);
+      const uint32_t acc = tmem + (uint32_t)(2 * Cfg::A_COLS + (j & 1) * N);
 #pragma unroll
-            for (int sk = 0; sk < Cfg::KSTEPS / 2; ++sk) {
-              const int st = kh * (Cfg::KSTEPS / 2) + sk;
-              const uint32_t kbo = (uint32_t)((st >> 2) * N * 128 + (st & 3) * 32) + hoff;
-              tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
-              tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bl + kbo), idesc, 1u);
-              tc_mma_tf32_ts(acc, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
-            }
-            if (kh == 1) tc_commit(smem_u32(&bar_mma[u % AR]));
-          }
-          if (ok) tc_commit(smem_u32(&bar_a_free[kh]));
-        }
+      for (int st = 0; st < Cfg::KSTEPS; ++st) {
+        // K step st: 16 fp16 = 8 A columns; in B, 32 bytes of a 128-byte atom
+        const uint32_t kbo = (uint32_t)((st >> 2) * N * 128 + (st & 3) * 32);
+        tc_mma_f16_ts(acc, ah + 8 * st, sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
+        tc_mma_f16_ts(acc, ah + 8 * st, sw128_desc(bl + kbo), idesc, 1u);
+        tc_mma_f16_ts(acc, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
       }
-    }
-    for (uint64_t j = 0; j < count && ok && !Cfg::SPLIT; ++j) {
-      if (!wait(&bar_a_ready[j % Cfg::A_BUFS], (uint32_t)((j / Cfg::A_BUFS) & 1))) break;
-      const uint32_t ah = tmem + (uint32_t)((j % Cfg::A_BUFS) * Cfg::A_COLS);
-      const uint32_t al = ah + (uint32_t)K;
-      for (int h = 0; h < Cfg::PASSES; ++h) {
-        const uint64_t u = j * Cfg::PASSES + h;
-        if (u >= 2 && !wait(&bar_acc_free[u & 1], (uint32_t)(((u >> 1) - 1) & 1))) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t acc = tmem + (uint32_t)(Cfg::A_BUFS * Cfg::A_COLS + (u & 1) * Cfg::ACC_COLS);
-        // this pass's B rows (output columns) h*NH .. h*NH+NH-1: whole 8-row
-        // groups of each 128-byte K atom, so only the start address moves
-        const uint32_t hoff = (uint32_t)(h * Cfg::NH * 128);
-#pragma unroll
-        for (int st = 0; st < Cfg::KSTEPS; ++st) {
-          const uint32_t kbo = (uint32_t)((st >> 2) * N * 128 + (st & 3) * 32) + hoff;
-          // main term hi*hi in its own accumulator; the two correction terms
-          // (2^-11 smaller) in a second one, summed in FP32 by the epilogue
-          tc_mma_tf32_ts(acc, ah + 8 * st, sw128_desc(bh + kbo), idesc, st > 0 ? 1u : 0u);
-          tc_mma_tf32_ts(acc + Cfg::NH, ah + 8 * st, sw128_desc(bl + kbo), idesc, st > 0 ? 1u : 0u);
-          tc_mma_tf32_ts(acc + Cfg::NH, al + 8 * st, sw128_desc(bh + kbo), idesc, 1u);
-        }
-        tc_commit(smem_u32(&bar_mma[u & 1]));
-      }
+      tc_commit(smem_u32(&bar_mma[j & 1]));
     }
   }
   tc_fence_before();
@@ -1061,7 +959,7 @@ int encode_half_tiles(const State* st, const Pass& p, TcGeom& g, CUtensorMap* ma
         if ((c >> b) & 1) off |= 8u << jb;
         ++b;
       }
-    g.ctile[c] = off;
+    g.ctile[c] = off ^ ((off >> 3) & 0x70u);  // swizzled (see the converters)
   }
   for (int b = 0, jb = 0; jb < TBH; ++jb)
     if (!hg.is_target[jb]) g.gbit_off[b++] = 8u << jb;
@@ -1090,7 +988,7 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
           if ((c >> b) & 1) off |= 8u << jb;
           ++b;
         }
-      g.ctile[c] = off;
+      g.ctile[c] = off ^ ((off >> 3) & 0x70u);  // swizzled (see the converters)
     }
   }
   static int attr_done[64] = {0};
@@ -1109,30 +1007,59 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   KB_CUDA(cudaGetLastError());
 }
 
-uint32_t host_tf32_rna(float x) {
-  uint32_t u;
-  std::memcpy(&u, &x, 4);
-  if ((u & 0x7f800000u) == 0x7f800000u) return u & 0xffffe000u;  // inf / nan: truncate
-  u += 0x1000u;  // round half away from zero on the magnitude
-  return u & 0xffffe000u;
+// IEEE binary16 bits of v, rounded to nearest, ties to even (host only).
+uint16_t host_f16_bits(double v) {
+  const uint16_t sign = std::signbit(v) ? 0x8000u : 0u;
+  const double a = std::fabs(v);
+  if (a == 0) return sign;
+  if (!(a < 65520.0)) return (uint16_t)(sign | 0x7c00u);  // rounds to infinity
+  int ex;
+  std::frexp(a, &ex);  // a in [2^(ex-1), 2^ex)
+  int e = ex - 1;
+  if (e < -14) e = -14;  // subnormals: spacing 2^-24
+  double m = std::nearbyint(std::ldexp(a, 10 - e));  // significand in units of 2^(e-10)
+  if (m >= 2048) {
+    m /= 2;
+    ++e;
+  }
+  if (e > 15) return (uint16_t)(sign | 0x7c00u);
+  if (m < 1024) return (uint16_t)(sign | (uint16_t)m);  // subnormal (e = -14)
+  return (uint16_t)(sign | ((e + 15) << 10) | ((int)m - 1024));
+}
+
+double host_f16_value(uint16_t h) {
+  const int ex = (h >> 10) & 31, man = h & 1023;
+  const double v = ex == 0 ? std::ldexp((double)man, -24) : std::ldexp((double)(1024 + man), ex - 25);
+  return (h & 0x8000u) ? -v : v;
 }
 
 }  // namespace
 
 bool tc_supported(int k) { return k >= 4 && k <= 6; }
 
+// hi and lo images of whole 128-byte atoms along K, then the scale word
 size_t tc_image_bytes(int k) {
   const size_t dim = size_t{1} << k;
-  return 2 * (2 * dim) * (2 * dim) * 4;
+  return 2 * ((2 * dim + 63) / 64) * (2 * dim) * 128 + 16;
 }
 
-// B = real embedding of mat (row-major dim x dim complex), stored as the
-// K-major SW128 images hi then lo (N rows of K floats each).
+// B = real embedding of mat (row-major dim x dim complex) scaled by 2^sb
+// (its largest entry into [2^14, 2^15)), stored as the K-major SW128 fp16
+// images hi then lo (N rows of K halves each), then sb as a 32-bit integer.
 void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& out) {
   const int dim = 1 << k, K = 2 * dim, N = 2 * dim;
   out.assign(tc_image_bytes(k) / 4, 0u);
+  double maxb = 0;
+  for (const cplx& m : mat) maxb = std::max(maxb, std::max(std::fabs(m.real()), std::fabs(m.imag())));
+  int sb = 14;
+  if (maxb > 0) {
+    int ex;
+    std::frexp(maxb, &ex);  // maxb in [2^(ex-1), 2^ex)
+    sb = std::max(-24, std::min(24, 15 - ex));
+  }
+  const size_t img = (tc_image_bytes(k) - 16) / 2;
   unsigned char* hi = reinterpret_cast<unsigned char*>(out.data());
-  unsigned char* lo = hi + (size_t)N * K * 4;
+  unsigned char* lo = hi + img;
   for (int n = 0; n < N; ++n)
     for (int kk = 0; kk < K; ++kk) {
       const int r = n >> 1, c = kk >> 1;
@@ -1140,18 +1067,16 @@ void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& 
       double v;
       if ((n & 1) == 0) v = (kk & 1) == 0 ? m.real() : -m.imag();
       else v = (kk & 1) == 0 ? m.imag() : m.real();
-      const float f = (float)v;
-      const uint32_t h = host_tf32_rna(f);
-      float hf;
-      std::memcpy(&hf, &h, 4);
-      const float l = f - hf;
-      uint32_t lu;
-      std::memcpy(&lu, &l, 4);
-      lu = host_tf32_rna(l);  // unbiased: the tensor core would truncate it
-      const uint32_t off = sw128_offset(n, kk, N);
-      std::memcpy(hi + off, &h, 4);
-      std::memcpy(lo + off, &lu, 4);
+      v = std::ldexp(v, sb);
+      const uint16_t h = host_f16_bits(v);
+      const uint16_t l = host_f16_bits(v - host_f16_value(h));
+      const uint32_t off = sw128_offset_h(n, kk, N);
+      if (off + 2 > img) fail(KETGPU_ERR_LOGIC, "tensor-core image layout");
+      std::memcpy(hi + off, &h, 2);
+      std::memcpy(lo + off, &l, 2);
     }
+  const int32_t sbw = sb;
+  std::memcpy(lo + img, &sbw, 4);
 }
 
 void launch_fused_tc(const State& s, const Pass& p, const void* b_image) {

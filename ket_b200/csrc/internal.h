@@ -114,7 +114,7 @@ struct Plan {
   std::vector<Pass> passes;
   std::vector<std::vector<cplx>> matrices;  // FP64 block matrices (host)
   // device copies, built lazily per device: FP64 (c128 SIMT), FP32 (c64 SIMT),
-  // tcgen05 B operands (hi/lo TF32 images in the shared-memory layout)
+  // tcgen05 B operands (hi/lo fp16 images in the shared-memory layout)
   void* d_mat64 = nullptr;
   void* d_mat32 = nullptr;
   void* d_tc = nullptr;

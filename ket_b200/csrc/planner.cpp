@@ -229,7 +229,11 @@ PlanOptions resolve_options(const ketgpu_options* opt) {
     fail(KETGPU_ERR_INVALID, "unknown fusion mode");
   o.precision = opt->precision;
   o.fusion = opt->fusion;
-  o.max_k = opt->max_block_qubits ? opt->max_block_qubits : 5;
+  // default block size: 6 qubits for complex64 on the tensor cores (their
+  // 3xFP16 blocks stay memory-bound at k = 6, so fewer passes win), 5 for
+  // the SIMT blocks, whose arithmetic grows with 2^k per amplitude
+  o.max_k = opt->max_block_qubits ? opt->max_block_qubits
+                                  : (opt->precision == KETGPU_C64 && opt->tensor_cores ? 6 : 5);
   if (o.max_k < 1 || o.max_k > 6) fail(KETGPU_ERR_INVALID, "max_block_qubits must be in [1, 6]");
   o.tensor = opt->tensor_cores != 0;
   o.renormalize = opt->renormalize;
