@@ -17,6 +17,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -530,6 +531,46 @@ void emit_diagonal(Plan& plan, int n, const ketgpu_op* ops, const Block& b) {
   plan.passes.push_back(p);
 }
 
+// Block matrices of the plan being built on this thread: emit_fused records
+// each one as a job and build_plan computes them all at the end, in
+// parallel (at k = 6 they are most of the planning time).
+struct MatrixJob {
+  size_t index;
+  std::vector<int> gates;
+  std::vector<int> qubits;
+};
+thread_local std::vector<MatrixJob>* t_matrix_jobs = nullptr;
+
+void compute_matrices(Plan& plan, const ketgpu_op* ops, const std::vector<MatrixJob>& jobs) {
+  auto work = [&](const MatrixJob& jb) {
+    std::vector<const ketgpu_op*> gs;
+    for (int gi : jb.gates) gs.push_back(&ops[gi]);
+    plan.matrices[jb.index] = block_matrix(gs, jb.qubits.data(), (int)jb.qubits.size());
+  };
+  const unsigned nt = jobs.size() < 16 ? 1u
+                      : std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+  if (nt <= 1) {
+    for (const MatrixJob& jb : jobs) work(jb);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::exception_ptr err;
+  std::atomic<bool> failed{false};
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; ++t)
+    th.emplace_back([&] {
+      for (size_t i; (i = next.fetch_add(1)) < jobs.size();) {
+        try {
+          work(jobs[i]);
+        } catch (...) {
+          if (!failed.exchange(true)) err = std::current_exception();
+        }
+      }
+    });
+  for (auto& x : th) x.join();
+  if (err) std::rethrow_exception(err);
+}
+
 void emit_fused(Plan& plan, int n, const ketgpu_op* ops, const Block& b, const PlanOptions& opt) {
   std::vector<const ketgpu_op*> gs;
   for (int gi : b.gates) gs.push_back(&ops[gi]);
@@ -545,12 +586,12 @@ void emit_fused(Plan& plan, int n, const ketgpu_op* ops, const Block& b, const P
     std::sort(qs.begin(), qs.end());
   }
   const int k = (int)qs.size();
-  std::vector<cplx> mat = block_matrix(gs, qs.data(), k);
   Pass p;
   p.first_op = b.gates.front();
   p.n_gates = (int)b.gates.size();
   p.gates = b.gates;
   if (k == 1) {  // one 2x2 through the streaming pair kernel
+    const std::vector<cplx> mat = block_matrix(gs, qs.data(), k);
     p.kind = PassKind::Pair;
     p.mode = kPairGeneral;
     p.nfixed = 1;
@@ -566,7 +607,12 @@ void emit_fused(Plan& plan, int n, const ketgpu_op* ops, const Block& b, const P
   for (int j = 0; j < k; ++j) p.qubits[j] = qs[j];
   p.tensor = block_on_tensor_cores(n, k, opt);
   p.mat_index = plan.matrices.size();
-  plan.matrices.push_back(std::move(mat));
+  if (t_matrix_jobs) {
+    plan.matrices.emplace_back();
+    t_matrix_jobs->push_back({p.mat_index, b.gates, qs});
+  } else {
+    plan.matrices.push_back(block_matrix(gs, qs.data(), k));
+  }
   plan.passes.push_back(p);
 }
 
@@ -642,6 +688,11 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
   plan.ops.assign(ops, ops + nops);
   plan.passes.clear();
   plan.matrices.clear();
+  std::vector<MatrixJob> jobs;
+  struct JobScope {
+    explicit JobScope(std::vector<MatrixJob>* j) { t_matrix_jobs = j; }
+    ~JobScope() { t_matrix_jobs = nullptr; }
+  } job_scope(&jobs);
   uint64_t n_gates = 0;
   double predicted = 0;
   const size_t amp = opt.precision == KETGPU_C64 ? 8 : 16;
@@ -814,6 +865,8 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
     }
   }
   flush();
+  t_matrix_jobs = nullptr;
+  compute_matrices(plan, ops, jobs);
   bool any_tensor = false;
   for (const Pass& p : plan.passes) any_tensor |= p.tensor;
   if ((opt.renormalize == 0 && any_tensor) || (opt.renormalize > 0 && !plan.passes.empty())) {

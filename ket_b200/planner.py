@@ -271,9 +271,9 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
         # plans are built first, then timed in an order that alternates from
         # circuit to circuit (the plan timed second runs on a warmer GPU)
         CostModel.detach()
-        p_greedy = Plan(n, c.to_ops(), make_options("c64", "greedy", 5, True))
+        p_greedy = Plan(n, c.to_ops(), make_options("c64", "greedy", 0, True))  # library default k
         model.attach()
-        p_learned = Plan(n, c.to_ops(), make_options("c64", "learned", 5, True))
+        p_learned = Plan(n, c.to_ops(), make_options("c64", "learned", 0, True))
         CostModel.detach()
         st_ = _state(n)
         if i % 2 == 0:
@@ -282,10 +282,10 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
         else:
             t_learned = float(timed_execute(p_learned, st_).sum())
             t_greedy = float(timed_execute(p_greedy, st_).sum())
-        # the best fixed alternative: greedy growth with 6-qubit blocks
-        p_greedy6 = Plan(n, c.to_ops(), make_options("c64", "greedy", 6, True))
-        t_greedy6 = float(timed_execute(p_greedy6, st_).sum())
-        p_greedy6.close()
+        # the fixed alternative: greedy growth with 5-qubit blocks
+        p_greedy5 = Plan(n, c.to_ops(), make_options("c64", "greedy", 5, True))
+        t_greedy5 = float(timed_execute(p_greedy5, st_).sum())
+        p_greedy5.close()
         same = plan_signature(p_greedy) == plan_signature(p_learned)
         if not same:  # two more alternating timings of each plan, best of three
             st = _state(n)
@@ -294,7 +294,7 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
                 t_learned = min(t_learned, float(timed_execute(p_learned, st).sum()))
         pred_learned = float(p_learned.stats()["predicted_us"]) / 1e3
         row = {"n": n, "depth": d, "seed": s, "gates": int(p_greedy.stats()["n_gates"]),
-               "greedy_ms": t_greedy, "learned_ms": t_learned, "greedy6_ms": t_greedy6, "learned_pred_ms": pred_learned,
+               "greedy_ms": t_greedy, "learned_ms": t_learned, "greedy5_ms": t_greedy5, "learned_pred_ms": pred_learned,
                "greedy_passes": int(p_greedy.stats()["n_passes"]), "learned_passes": int(p_learned.stats()["n_passes"]),
                "same_plan": bool(same)}
         if i in unfused_set or i in check_set:
@@ -336,8 +336,8 @@ def main(argv: Optional[Sequence[str]] = None) -> None:
         "loss_curve": curve, "train_rmse_log_us": train_rmse,
         "eval_total_greedy_ms": float(gt.sum()), "eval_total_learned_ms": float(lt.sum()),
         "eval_learned_over_greedy": float(lt.sum() / gt.sum()),
-        "eval_learned_over_greedy_k6": float(lt.sum() / sum(r["greedy6_ms"] for r in rows)),
-        "eval_greedy_k6_over_greedy": float(sum(r["greedy6_ms"] for r in rows) / gt.sum()),
+        "eval_learned_over_greedy_k5": float(lt.sum() / sum(r["greedy5_ms"] for r in rows)),
+        "eval_greedy_k5_over_greedy": float(sum(r["greedy5_ms"] for r in rows) / gt.sum()),
         "eval_learned_over_greedy_geomean": float(np.exp(np.mean(np.log(lt / gt)))),
         "eval_same_plan_count": int(sum(r["same_plan"] for r in rows)),
         "eval_differing_plans": int(sum(not r["same_plan"] for r in rows)),

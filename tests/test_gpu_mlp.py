@@ -107,9 +107,9 @@ def test_trained_network_predicts_pass_times_better_than_the_static_model():
     for r in diff:
         c = random_mixed(r["n"], r["depth"], seed=r["seed"])
         pl.CostModel.detach()
-        pg = ket.Plan(r["n"], c.to_ops(), ket.make_options("c64", "greedy", 5, True))
+        pg = ket.Plan(r["n"], c.to_ops(), ket.make_options("c64", "greedy", 0, True))
         model.attach()
-        plr = ket.Plan(r["n"], c.to_ops(), ket.make_options("c64", "learned", 5, True))
+        plr = ket.Plan(r["n"], c.to_ops(), ket.make_options("c64", "learned", 0, True))
         pl.CostModel.detach()
         st = pl._state(r["n"])
         g = min(float(pl.timed_execute(pg, st).sum()) for _ in range(3))
