@@ -42,12 +42,12 @@ sys.path.insert(0, ROOT)
 N_QUBITS, DEPTH, SEED = 30, 40, 1234
 METRIC = "time per 30q circuit"
 
-# DRAM bytes (read + write) of one fused_tc_kernel<5> launch on a 2^26
-# complex64 state, from ncu (dram__bytes_read.sum 536.98 MB +
-# dram__bytes_write.sum 477.04 MB, one launch of the 26-qubit depth-4 brick
-# wall: the block on qubits 10..14).  A launch streams the state once, so the
+# DRAM bytes (read + write) of one fused_tc_kernel<k> launch on a 2^26
+# complex64 state, from ncu (dram__bytes_read.sum + dram__bytes_write.sum,
+# one dense block of the 26-qubit workload `--workload kernels26`; see
+# profiles/fused_tc_kernel6_26q.md).  A launch streams the state once, so the
 # figure scales with 2^n.
-TC_TRAFFIC_BYTES_26Q = 536.983808e6 + 477.042688e6
+TC_TRAFFIC_BYTES_26Q = {5: 536.966400e6 + 477.739776e6, 6: 537.047552e6 + 477.192448e6}
 
 
 def peaks():
@@ -552,14 +552,21 @@ def main():
     peak, peak_kind = peaks()
     roof = None
     if tc_idx:
-        dur = float(np.mean(per_pass[tc_idx]))
-        byts = float(np.mean([info[i][3] for i in tc_idx]))
+        # the dominant kernel: the block size most of the tensor-core passes have
+        ks = [info[i][1] for i in tc_idx]
+        kdom = max(set(ks), key=ks.count)
+        dom = [i for i in tc_idx if info[i][1] == kdom]
+        dur = float(np.mean(per_pass[dom]))
+        byts = float(np.mean([info[i][3] for i in dom]))
         ach = byts / (dur * 1e-3) / 1e9
+        traffic = TC_TRAFFIC_BYTES_26Q.get(kdom)
         roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "peak_source": peak_kind, "traffic": TC_TRAFFIC_BYTES_26Q * 2.0 ** (nq - 26),
+                "peak_source": peak_kind, "traffic": traffic * 2.0 ** (nq - 26) if traffic else None,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 26 qubits, "
-                                  "scaled by 2^(n-26)", "kernel": "fused_tc_kernel<5>",
-                "bytes_per_launch": byts, "mean_launch_ms": dur, "launches_per_step": len(tc_idx)}
+                                  "scaled by 2^(n-26)", "kernel": f"fused_tc_kernel<{kdom}>",
+                "bytes_per_launch": byts, "mean_launch_ms": dur, "launches_per_step": len(dom),
+                "tensor_passes_all_k": len(tc_idx),
+                "all_tensor_passes_gbs": float(np.mean([info[i][3] / (per_pass[i] * 1e-3) / 1e9 for i in tc_idx]))}
     other = [i for i in range(npass) if i not in tc_idx]
     pass_summary = {
         "dense_tc_ms": float(per_pass[tc_idx].sum()) if tc_idx else 0.0,

@@ -196,6 +196,7 @@ int ketgpu_run_last_profile(double* out6);
 int ketgpu_release_cache(void);
 
 /* ---- reductions (FP64 accumulation) --------------------------------- */
+/* *out = sum over x of |amplitude x|^2 (the squared norm). */
 int ketgpu_norm(const ketgpu_state* s, double* out);
 /* <a|b> (complex) -- fidelity checks. */
 int ketgpu_inner(const ketgpu_state* a, const ketgpu_state* b, double* re, double* im);

@@ -117,7 +117,25 @@ struct TcGeom {
   int half;
   uint64_t top_off;
   uint32_t gbit_off[kGroupBits];
+  // non-null: the epilogue also sums |out|^2 in FP64 and CTA b writes its sum
+  // to norm_out[b]
+  double* norm_out;
+  // cp.async producers and staged stores: chunk i of thread t covers tile
+  // amplitudes e = 2t + 256i and e + 1; its offsets are those of e = 2t
+  // XOR those of e = 256i (amp_offsets is XOR-linear in e), and these tables
+  // hold the latter: state offset, A-layout (input) and staging (output)
+  // byte offsets
+  uint64_t chunk_g[32];
+  uint32_t chunk_s_in[32], chunk_s_out[32];
 };
+
+// Output staging when qubit 0 is a group bit: amplitudes e and e+1 (rows
+// r and r+64, same combination c) side by side in one 16-byte slot, slot
+// (r mod 64) * dim + (c ^ (r mod 8)), so the store phase reads one 16-byte
+// word per chunk and the TMEM drain writes stay spread over the banks.
+__host__ __device__ inline uint32_t pair_slot_offset(int row, int comb, int dim) {
+  return (uint32_t)(((row & 63) * dim + (comb ^ (row & 7))) * 16 + 8 * (row >> 6));
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -146,6 +164,28 @@ __host__ __device__ __forceinline__ uint32_t sw128_offset_h(int row, int kk, int
   const int kb = kk >> 6;             // 64 fp16 per 128-byte atom row
   const int chunk = (kk & 63) >> 3;   // 16-byte chunk in the row
   return (uint32_t)(kb * rows * 128 + row * 128 + ((chunk ^ (row & 7)) << 4) + ((kk & 7) << 1));
+}
+
+// Offsets of tile amplitude e (address order: bit j of e <-> qubit
+// tile_pos[j]): from the tile base in the state (goff), and in bytes in an
+// A-layout image (soff: row = group, with a group bit at qubit 0 rotated to
+// row bit 6, kk = 2*comb), or with out_layout and qubit 0 a group bit in the
+// paired output staging.  Both are XOR-linear in e: e's bits land on
+// disjoint positions, and the swizzles XOR disjoint fields.
+__host__ __device__ inline void amp_offsets(const TcGeom& g, int tb, int dim, int e, bool out_layout,
+                                            uint64_t* goff, uint32_t* soff) {
+  const bool q0_group = !g.is_target[0];
+  uint64_t off = 0;
+  int grp = 0, comb = 0, gb = 0, cb = 0;
+  for (int j = 0; j < tb; ++j) {
+    const int bit = (e >> j) & 1;
+    if (g.is_target[j]) comb |= bit << cb++;
+    else grp |= bit << gb++;
+    if (bit) off |= uint64_t{1} << g.tile_pos[j];
+  }
+  const int row = q0_group ? ((grp >> 1) | ((grp & 1) << (kGroupBits - 1))) : grp;
+  *goff = off;
+  *soff = (out_layout && q0_group) ? pair_slot_offset(row, comb, dim) : sw128_offset(row, 2 * comb, 128);
 }
 
 __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
@@ -275,7 +315,10 @@ __host__ __device__ constexpr uint32_t f16_idesc() {
 constexpr int kProducers = 128, kConverters = 128, kEpilogue = 128;
 constexpr int kScaleRing = 4;  // row scales in flight (see the converters)
 
-template <int KQ>
+// NORM: the epilogue also sums |out|^2 into g.norm_out (the plan's last
+// block before its norm restore); a separate instantiation, so the common
+// one carries none of it.
+template <int KQ, bool NORM>
 __global__ void __launch_bounds__(kTcThreads, 1)
     fused_tc_kernel(float2* __restrict__ s, TcGeom g, const uint32_t* __restrict__ bimg,
                     const __grid_constant__ CUtensorMap tmap) {
@@ -308,6 +351,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __shared__ uint64_t base_ring[R];
   // Per tile and TMEM lane: s + sb, the exponent the epilogue scales by.
   __shared__ int8_t row_exp[kScaleRing][128];
+  __shared__ double norm_sh[4];
   __shared__ volatile int abort_flag;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -387,38 +431,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   };
 
-  // Chunk offsets shared by producers and epilogue threads: chunk
-  // ch = t + 128*i covers tile amplitudes e = 2ch, 2ch+1 (address order, bit j
-  // of e <-> qubit g.tile_pos[j]); goff = offset of e in the state from the
-  // tile base, soff = byte offset of e in an A-layout image (row = group with
-  // a group bit at qubit 0 rotated to row bit 6, kk = 2*comb).  Amplitude e+1
-  // sits at soff + 8 (qubit 0 is the lowest target: next combination) or at
-  // soff + 8192 (qubit 0 is a group bit: row + 64).
+  // Chunk i of producer / epilogue thread t covers tile amplitudes
+  // e = 2t + 256i and e + 1: amplitude e+1 sits at soff + 8 (qubit 0 is the
+  // lowest target: next combination) or at soff + 8192 (qubit 0 is a group
+  // bit: row + 64).  Offsets: this thread's (e = 2t) XOR the chunk table's.
   const uint32_t pair_step = q0_group ? 64u * 128u : 8u;
-  // Output staging when qubit 0 is a group bit: amplitudes e and e+1 (rows
-  // r and r+64, same combination c) side by side in one 16-byte slot, slot
-  // (r mod 64) * DIM + (c ^ (r mod 8)), so the store phase reads one 16-byte
-  // word per chunk and the TMEM drain writes stay spread over the banks.
-  auto pair_slot = [](int row, int comb) -> uint32_t {
-    return (uint32_t)(((row & 63) * DIM + (comb ^ (row & 7))) * 16 + 8 * (row >> 6));
-  };
-  auto chunk_offsets = [&](int t, uint64_t* goff, uint32_t* soff, bool out_layout) {
-#pragma unroll
-    for (int i = 0; i < CPT; ++i) {
-      const int e = 2 * (t + kProducers * i);
-      uint64_t off = 0;
-      int grp = 0, comb = 0, gb = 0, cb = 0;
-      for (int j = 0; j < Cfg::TB; ++j) {
-        const int bit = (e >> j) & 1;
-        if (g.is_target[j]) comb |= bit << cb++;
-        else grp |= bit << gb++;
-        if (bit) off |= uint64_t{1} << g.tile_pos[j];
-      }
-      const int row = q0_group ? ((grp >> 1) | ((grp & 1) << (kGroupBits - 1))) : grp;
-      goff[i] = off;
-      soff[i] = (out_layout && q0_group) ? pair_slot(row, comb) : sw128_offset(row, 2 * comb, 128);
-    }
-  };
+  auto pair_slot = [](int row, int comb) -> uint32_t { return pair_slot_offset(row, comb, DIM); };
   auto tile_base = [&](uint64_t t) -> uint64_t {
     uint64_t b = t << g.m_low;
     for (int j = 0; j < g.nh; ++j) {
@@ -462,9 +480,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   } else if (warp < 4) {
     // ------------------------------------------------------------ producers
-    uint64_t goff[CPT];
-    uint32_t soff[CPT];
-    chunk_offsets(tid, goff, soff, false);
+    uint64_t g0;
+    uint32_t s0;
+    amp_offsets(g, Cfg::TB, DIM, 2 * tid, false, &g0, &s0);
     for (uint64_t j = 0; j < count; ++j) {
       const int slot = (int)(j % S);
       if (j >= (uint64_t)S && !wait(&bar_free[slot], (uint32_t)(((j / S) - 1) & 1))) break;
@@ -473,11 +491,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const float2* src = s + base;
 #pragma unroll
       for (int i = 0; i < CPT; ++i) {
+        const uint64_t go = g0 ^ g.chunk_g[i];
+        const uint32_t so = s0 ^ g.chunk_s_in[i];
         if (q0_group) {
-          cp_async8(dst + soff[i], src + goff[i]);
-          cp_async8(dst + soff[i] + pair_step, src + goff[i] + 1);
+          cp_async8(dst + so, src + go);
+          cp_async8(dst + so + pair_step, src + go + 1);
         } else {
-          cp_async16(dst + soff[i], src + goff[i]);
+          cp_async16(dst + so, src + go);
         }
       }
       asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&bar_full[slot]))
@@ -617,6 +637,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int q = warp & 3;
     const int row = 32 * q + lane;
     const uint32_t acc_lane = tmem + (uint32_t)(2 * Cfg::A_COLS) + ((uint32_t)(32 * q) << 16);
+    double nacc = 0.0;  // this thread's sum of |out|^2 (g.norm_out)
     // Waits for tile j's accumulator and row scale; returns 2^-(s + sb).
     auto tile_ready = [&](uint64_t j, float* unscale) -> bool {
       if (!wait(&bar_mma[j & 1], (uint32_t)((j >> 1) & 1))) return false;
@@ -648,15 +669,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tmem_ld<16>(acc + (uint32_t)(part * 16), v);
           tmem_ld_wait();
 #pragma unroll
-          for (int i = 0; i < 8; ++i) dst[g.cdep[part * 8 + i]] = make_float2(v[2 * i] * us, v[2 * i + 1] * us);
+          for (int i = 0; i < 8; ++i) {
+            const float2 o = make_float2(v[2 * i] * us, v[2 * i + 1] * us);
+            dst[g.cdep[part * 8 + i]] = o;
+            if constexpr (NORM) nacc = fma((double)o.x, (double)o.x, fma((double)o.y, (double)o.y, nacc));
+          }
         }
         tc_fence_before();
         arrive(&bar_acc_free[j & 1]);
       }
     } else {
-      uint64_t goff[CPT];
-      uint32_t soff[CPT];
-      chunk_offsets(t, goff, soff, true);
+      uint64_t g0;
+      uint32_t s0;
+      amp_offsets(g, Cfg::TB, DIM, 2 * t, true, &g0, &s0);
       for (uint64_t j = 0; j < count; ++j) {
         const int slot = (int)(j % S);
         unsigned char* out = raw + slot * Cfg::RAW_BYTES;
@@ -669,7 +694,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tmem_ld<16>(acc + (uint32_t)(part * 16), v);
           tmem_ld_wait();
 #pragma unroll
-          for (int i = 0; i < 16; ++i) v[i] *= us;
+          for (int i = 0; i < 16; ++i) {
+            v[i] *= us;
+            if constexpr (NORM) nacc = fma((double)v[i], (double)v[i], nacc);
+          }
           if (q0_group) {
 #pragma unroll
             for (int i = 0; i < 8; ++i)
@@ -687,9 +715,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         float2* dst = s + base_ring[j % R];
 #pragma unroll
         for (int i = 0; i < CPT; ++i)
-          *reinterpret_cast<float4*>(dst + goff[i]) = *reinterpret_cast<const float4*>(out + soff[i]);
+          *reinterpret_cast<float4*>(dst + (g0 ^ g.chunk_g[i])) =
+              *reinterpret_cast<const float4*>(out + (s0 ^ g.chunk_s_out[i]));
         arrive(&bar_free[slot]);
       }
+    }
+    if constexpr (NORM) {
+      // the epilogue warps' sums, in a fixed order: warp, then warp 8..11
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) nacc += __shfl_xor_sync(0xffffffffu, nacc, o);
+      if (lane == 0) norm_sh[q] = nacc;
+      asm volatile("bar.sync 2, %0;" ::"n"(kEpilogue) : "memory");
+      if (t == 0) g.norm_out[blockIdx.x] = (norm_sh[0] + norm_sh[1]) + (norm_sh[2] + norm_sh[3]);
     }
   } else if (warp == 12 && lane == 0) {
     // ------------------------------------------------------------ MMA issue
@@ -911,6 +948,17 @@ void tile_geometry(int n, const Pass& p, TcGeom& g) {
   g.nh = 0;
   for (int i = g.m_low; i < Cfg::TB; ++i) g.hpos[g.nh++] = g.tile_pos[i];
   g.n_tiles = (uint64_t{1} << n) >> Cfg::TB;
+  constexpr int CPT = Cfg::TILE / 2 / 128;
+  static_assert(CPT <= 32, "chunk tables");
+  for (int i = 0; i < CPT; ++i) {
+    uint64_t go;
+    uint32_t si, so;
+    amp_offsets(g, Cfg::TB, Cfg::DIM, 256 * i, false, &go, &si);
+    amp_offsets(g, Cfg::TB, Cfg::DIM, 256 * i, true, &go, &so);
+    g.chunk_g[i] = go;
+    g.chunk_s_in[i] = si;
+    g.chunk_s_out[i] = so;
+  }
 }
 
 // The half tile of a k = 6 block (host only): the tile less its highest
@@ -967,10 +1015,13 @@ int encode_half_tiles(const State* st, const Pass& p, TcGeom& g, CUtensorMap* ma
 }
 
 template <int KQ>
-void launch_tc(const State& st, const Pass& p, const void* b_image) {
+void launch_tc(const State& st, const Pass& p, const void* b_image, double* norm_partials) {
   using Cfg = TcCfg<KQ>;
   TcGeom g;
   tile_geometry<KQ>(st.n, p, g);
+  g.norm_out = norm_partials;
+  if (norm_partials)  // entries past the grid stay zero for the in-order sum
+    KB_CUDA(cudaMemsetAsync(norm_partials, 0, sizeof(double) * kNormBlocks, st.stream));
   CUtensorMap tmap;
   std::memset(&tmap, 0, sizeof(tmap));
   // Tensor-copy blocks (qubit 0 a group bit) always store directly.
@@ -993,7 +1044,9 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   }
   static int attr_done[64] = {0};
   if (st.device >= 0 && st.device < 64 && !(attr_done[st.device] & (1 << KQ))) {
-    KB_CUDA(cudaFuncSetAttribute(fused_tc_kernel<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    KB_CUDA(cudaFuncSetAttribute(fused_tc_kernel<KQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Cfg::SMEM));
+    KB_CUDA(cudaFuncSetAttribute(fused_tc_kernel<KQ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)Cfg::SMEM));
     attr_done[st.device] |= 1 << KQ;
   }
@@ -1001,8 +1054,13 @@ void launch_tc(const State& st, const Pass& p, const void* b_image) {
   if (!sms[st.device]) sms[st.device] = sm_count_tc(st.device);
   uint64_t grid = (uint64_t)sms[st.device];
   if (grid > g.n_tiles) grid = g.n_tiles;
-  fused_tc_kernel<KQ><<<(unsigned)grid, kTcThreads, Cfg::SMEM, st.stream>>>(
-      static_cast<float2*>(st.amps), g, static_cast<const uint32_t*>(b_image), tmap);
+  if (norm_partials && grid > (uint64_t)kNormBlocks) fail(KETGPU_ERR_LOGIC, "tensor-core norm partials");
+  if (norm_partials)
+    fused_tc_kernel<KQ, true><<<(unsigned)grid, kTcThreads, Cfg::SMEM, st.stream>>>(
+        static_cast<float2*>(st.amps), g, static_cast<const uint32_t*>(b_image), tmap);
+  else
+    fused_tc_kernel<KQ, false><<<(unsigned)grid, kTcThreads, Cfg::SMEM, st.stream>>>(
+        static_cast<float2*>(st.amps), g, static_cast<const uint32_t*>(b_image), tmap);
   count_launch();
   KB_CUDA(cudaGetLastError());
 }
@@ -1079,10 +1137,10 @@ void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& 
   std::memcpy(lo + img, &sbw, 4);
 }
 
-void launch_fused_tc(const State& s, const Pass& p, const void* b_image) {
-  if (p.k == 5) launch_tc<5>(s, p, b_image);
-  else if (p.k == 4) launch_tc<4>(s, p, b_image);
-  else if (p.k == 6) launch_tc<6>(s, p, b_image);
+void launch_fused_tc(const State& s, const Pass& p, const void* b_image, double* norm_partials) {
+  if (p.k == 5) launch_tc<5>(s, p, b_image, norm_partials);
+  else if (p.k == 4) launch_tc<4>(s, p, b_image, norm_partials);
+  else if (p.k == 6) launch_tc<6>(s, p, b_image, norm_partials);
   else fail(KETGPU_ERR_LOGIC, "tensor-core block supports k = 4, 5 or 6");
 }
 

@@ -587,8 +587,11 @@ double Pass::bytes(int n, size_t amp) const {
   return 2.0 * amp * 2.0 * dim / (double)(uint64_t{1} << nfixed);
 }
 
+__global__ void store_one_kernel(double* p) { *p = 1.0; }
+
 void set_ground(const State& s) {
   s.touch();
+  s.ground_version = s.version;
   KB_CUDA(cudaMemsetAsync(s.amps, 0, s.dim() * s.amp_bytes(), s.stream));
   if (s.precision == KETGPU_C64)
     set_one_kernel<float><<<1, 1, 0, s.stream>>>(static_cast<float2*>(s.amps));
@@ -599,13 +602,23 @@ void set_ground(const State& s) {
 }
 
 void launch_pass(const State& s, const Plan& plan, const Pass& p) {
+  const bool ground = s.version == s.ground_version;
   s.touch();
   if (p.kind == PassKind::NormCapture) {
-    norm_to_device(s, plan.d_norm + 2, plan.d_norm);
+    if (ground) {  // |0...0>: the squared norm is 1, no pass over the state
+      store_one_kernel<<<1, 1, 0, s.stream>>>(plan.d_norm);
+      count_launch();
+      KB_CUDA(cudaGetLastError());
+    } else {
+      norm_to_device(s, plan.d_norm + 2, plan.d_norm);
+    }
     return;
   }
   if (p.kind == PassKind::NormRestore) {
-    norm_to_device(s, plan.d_norm + 2, plan.d_norm + 1);
+    if (p.norm_out)  // the block before summed |out|^2 per CTA into the partials
+      norm_from_partials(s, plan.d_norm + 2, plan.d_norm + 1);
+    else
+      norm_to_device(s, plan.d_norm + 2, plan.d_norm + 1);
     rescale_state(s, plan.d_norm, plan.d_norm + 1);
     return;
   }
@@ -627,7 +640,8 @@ void launch_pass(const State& s, const Plan& plan, const Pass& p) {
   if (s.precision == KETGPU_C128) {
     launch_fused_simt<double>(s, p, static_cast<const char*>(plan.d_mat64) + plan.off64[p.mat_index]);
   } else if (p.tensor) {
-    launch_fused_tc(s, p, static_cast<const char*>(plan.d_tc) + plan.offtc[p.mat_index]);
+    launch_fused_tc(s, p, static_cast<const char*>(plan.d_tc) + plan.offtc[p.mat_index],
+                    p.norm_out ? plan.d_norm + 2 : nullptr);
   } else {
     launch_fused_simt<float>(s, p, static_cast<const char*>(plan.d_mat32) + plan.off32[p.mat_index]);
   }

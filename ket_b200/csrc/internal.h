@@ -52,6 +52,9 @@ struct State {
   mutable double* tree = nullptr;
   mutable uint64_t tree_doubles = 0;
   mutable uint64_t tree_version = ~uint64_t{0};
+  // version right after set_ground: while version still equals it, the state
+  // is |0...0> and its squared norm is exactly 1
+  mutable uint64_t ground_version = ~uint64_t{0};
   uint64_t dim() const { return uint64_t{1} << n; }
   size_t amp_bytes() const { return precision == KETGPU_C64 ? 8 : 16; }
   void touch() const { ++version; }
@@ -89,6 +92,10 @@ struct Pass {
   int qubits[6] = {0, 0, 0, 0, 0, 0};  // sorted ascending; matrix bit b <-> qubits[b]
   size_t mat_index = 0;                // into Plan::matrices
   bool tensor = false;                 // tcgen05 path
+  // tcgen05 block directly before the plan's NormRestore: it also writes
+  // per-CTA FP64 sums of |out|^2 into the plan's norm partials, and the
+  // restore (norm_out set there too) takes the norm from them
+  bool norm_out = false;
   size_t diag_index = 0;               // Diagonal: into Plan::diags
   size_t run_index = 0;                // SharedRun: into Plan::runs
   int first_op = 0, n_gates = 0;       // provenance
@@ -169,7 +176,9 @@ void learned_predict(const std::vector<float>& rows, std::vector<float>& us);
 // ---- kernel launchers (gates.cu / fused_tc.cu / reduce.cu) -----------------
 void launch_pass(const State& s, const Plan& plan, const Pass& p);
 void upload_plan_matrices(Plan& plan, int device);
-void launch_fused_tc(const State& s, const Pass& p, const void* b_image);
+// norm_partials: null, or kNormBlocks doubles that receive the per-CTA sums
+// of |out|^2 (zero beyond the grid).
+void launch_fused_tc(const State& s, const Pass& p, const void* b_image, double* norm_partials = nullptr);
 // Host only: the producer and epilogue forms a tensor-core launch of pass p
 // on an n-qubit state takes (tma_dims = tensor-map dimensions, 0 for the
 // cp.async producers; direct = register-to-HBM stores), given the tensor-map
@@ -193,6 +202,8 @@ bool tc_supported(int k);
 void set_ground(const State& s);
 // Squared norm into a device scalar (partials: kNormBlocks doubles).
 void norm_to_device(const State& s, double* partials, double* out);
+// The same from partials a tensor-core block already wrote (in index order).
+void norm_from_partials(const State& s, const double* partials, double* out);
 // Look up (and so load) the no-allocation entry point's scratch array and
 // kernels on `device`, which must be current; once per device, at the first
 // state created there.

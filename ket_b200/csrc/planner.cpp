@@ -873,6 +873,11 @@ void build_plan(Plan& plan, int n, const ketgpu_op* ops, uint64_t nops, const Pl
     Pass cap, res;
     cap.kind = PassKind::NormCapture;
     res.kind = PassKind::NormRestore;
+    // a tensor-core block right before the restore sums the norm as it stores
+    if (!plan.passes.empty() && plan.passes.back().kind == PassKind::Fused && plan.passes.back().tensor) {
+      plan.passes.back().norm_out = true;
+      res.norm_out = true;
+    }
     plan.passes.insert(plan.passes.begin(), cap);
     plan.passes.push_back(res);
   }

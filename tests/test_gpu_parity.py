@@ -181,6 +181,40 @@ def test_norm_and_inner():
     assert abs(a.inner(b) - 1) < 1e-12
 
 
+@pytest.mark.parametrize("k", [4, 5, 6])
+def test_tensor_core_plans_keep_the_norm(k):
+    """The norm capture / restore around tensor-core blocks: from a reset
+    state (no capture pass: the norm is 1) and from an uploaded state of
+    norm 4 (captured), the final norm equals the starting one, whether the
+    restore sums the state itself or takes the last block's per-CTA sums;
+    n from one tile (k + 7 qubits) up."""
+    import ket_b200 as kb
+    from ket_b200.workloads import random_brickwork
+    for n in (k + 7, 16, 20):
+        c = random_brickwork(n, 8, seed=n + k)
+        opt = kb.make_options("c64", "greedy", k, True)
+        plan = kb.Plan(n, c.to_ops(), opt)
+        kinds = [plan.pass_info(i)["kind"] for i in range(int(plan.stats()["n_passes"]))]
+        assert kinds[0] == 3 and kinds[-1] == 3  # NormCapture ... NormRestore
+        plan.close()
+        d = kb.run_device(c, options=opt)
+        ref = kb.run_device(c, "c128")
+        # bound: FP32 rounding of the rescaled amplitudes (~2^-24 / sqrt(2^n));
+        # a CTA's partial missing from the sum would be off by 1/grid or more
+        assert abs(d.norm() - 1.0) < 1e-7, (n, d.norm())
+        assert fidelity(d.to_numpy(), ref.to_numpy()) > 1 - FID32
+        # an uploaded state of norm 4 keeps its norm through the same circuit
+        start = ref.to_numpy() * 2.0
+        u = kb.DeviceState(n, "c64").from_numpy(start)
+        u.apply(c, opt)
+        assert abs(u.norm() / 4.0 - 1.0) < 1e-7, (n, u.norm())
+        v = kb.DeviceState(n, "c128").from_numpy(start)
+        v.apply(c, kb.make_options("c128", "greedy", 5, True))
+        assert fidelity(u.to_numpy(), v.to_numpy()) > 1 - FID32
+        for x in (d, ref, u, v):
+            x.close()
+
+
 def test_sampler_bit_exact_against_oracle(oracle, golden):
     import ket_b200 as kb
     s10 = golden("random_mixed")["state_10"]
