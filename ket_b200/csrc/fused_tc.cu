@@ -188,6 +188,29 @@ __host__ __device__ inline void amp_offsets(const TcGeom& g, int tb, int dim, in
   *soff = (out_layout && q0_group) ? pair_slot_offset(row, comb, dim) : sw128_offset(row, 2 * comb, 128);
 }
 
+// Packed FP32 pairs (sm_100 f32x2 instructions: two FP32 operations each).
+using f32x2 = unsigned long long;
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float2 unpack2(f32x2 v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ f32x2 mul_x2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 fma_x2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
 }
@@ -600,6 +623,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         row_exp[j % kScaleRing][lane_row] = (int8_t)(sa + sb);
         arrive(&bar_scale[j % kScaleRing]);
         const float sc = __int_as_float((127 + sa) << 23);
+        const f32x2 sc2 = pack2(sc, sc), neg1 = pack2(-1.f, -1.f);
         const uint32_t areg = tmem + lane_off + (uint32_t)((j & 1) * Cfg::A_COLS);
 #pragma unroll
         for (int part = 0; part < K / 32; ++part) {
@@ -607,12 +631,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
             const float4 v = amp_pair(8 * part + i);
-            const float xs[4] = {v.x * sc, v.y * sc, v.z * sc, v.w * sc};
+            const f32x2 xs[2] = {mul_x2(pack2(v.x, v.y), sc2), mul_x2(pack2(v.z, v.w), sc2)};
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
-              const __half2 h = __floats2half2_rn(xs[2 * u], xs[2 * u + 1]);
+              const float2 x = unpack2(xs[u]);
+              const __half2 h = __floats2half2_rn(x.x, x.y);
               const float2 hf = __half22float2(h);
-              const __half2 l = __floats2half2_rn(xs[2 * u] - hf.x, xs[2 * u + 1] - hf.y);
+              const float2 r = unpack2(fma_x2(pack2(hf.x, hf.y), neg1, xs[u]));  // x - hi, exact
+              const __half2 l = __floats2half2_rn(r.x, r.y);
               hi[2 * i + u] = *reinterpret_cast<const uint32_t*>(&h);
               lo[2 * i + u] = *reinterpret_cast<const uint32_t*>(&l);
             }
@@ -662,6 +688,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // tile j's base is in the ring once its MMAs are done (the
         // producer wrote it before the tile's copy was even issued)
         float2* dst = s + base_ring[j % R] + gdep;
+        const f32x2 us2 = pack2(us, us);
         const uint32_t acc = acc_lane + (uint32_t)((j & 1) * N);
 #pragma unroll
         for (int part = 0; part < N / 16; ++part) {
@@ -670,7 +697,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tmem_ld_wait();
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            const float2 o = make_float2(v[2 * i] * us, v[2 * i + 1] * us);
+            const float2 o = unpack2(mul_x2(pack2(v[2 * i], v[2 * i + 1]), us2));
             dst[g.cdep[part * 8 + i]] = o;
             if constexpr (NORM) nacc = fma((double)o.x, (double)o.x, fma((double)o.y, (double)o.y, nacc));
           }
