@@ -51,7 +51,7 @@ void check(int rc) {
 }
 
 ketgpu_options options() {
-  ketgpu_options o{KETGPU_C128, KETGPU_FUSE_GREEDY, 5, 1, 0};
+  ketgpu_options o{KETGPU_C128, KETGPU_FUSE_GREEDY, 0, 1, 0};  // k: the library default
   if (const char* p = std::getenv("KET_B200_PRECISION"))
     o.precision = std::string(p) == "c64" ? KETGPU_C64 : KETGPU_C128;
   if (const char* f = std::getenv("KET_B200_FUSION")) {
