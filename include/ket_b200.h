@@ -167,6 +167,14 @@ int ketgpu_plan_pass_gates(const ketgpu_plan* p, uint64_t index, int32_t* gates,
  * no counterpart in ket. */
 int ketgpu_plan_pass_tc_form(const ketgpu_plan* p, uint64_t index, int32_t* tma_dims,
                              int32_t* direct);
+/* The tensor-core B operand of a k-qubit block (k = 4, 5 or 6) as plans
+ * upload it: the real embedding of `mat` (2^k x 2^k complex, row-major,
+ * interleaved re, im) scaled by 2^sb (its largest entry into [2^14, 2^15)),
+ * split into fp16 hi = round(x) and lo = round(x - hi), as two K-major
+ * 128-byte-swizzled images (hi, then lo, each in whole 128-byte atoms along
+ * K), then sb as a 32-bit integer.  Writes min(capacity, size) 32-bit words;
+ * *words receives the size.  Host only; no counterpart in ket. */
+int ketgpu_tc_image(int32_t k, const double* mat, uint32_t* out, uint64_t capacity, uint64_t* words);
 /* The state's CUDA stream (a cudaStream_t), for callers that order their
  * own work or events against the backend's. */
 void* ketgpu_state_stream(const ketgpu_state* s);

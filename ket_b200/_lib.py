@@ -52,7 +52,7 @@ class KetGpuTimeout(KetGpuError):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"ket_b200: {LIB_PATH} is missing; build it with `python -m ket_b200.build` "
+            f"ket_b200: {LIB_PATH} is missing; build it with `python ket_b200/build.py` "
             "(the backend has no CPU fallback)")
     L = ct.CDLL(LIB_PATH)
     vp, sz, i32, u32, u64 = ct.c_void_p, ct.c_size_t, ct.c_int32, ct.c_uint32, ct.c_uint64
@@ -82,6 +82,7 @@ def _load():
         "ketgpu_release_cache": ([], ct.c_int),
         "ketgpu_run_last_profile": ([vp], ct.c_int),
         "ketgpu_plan_pass_tc_form": ([vp, u64, ct.POINTER(i32), ct.POINTER(i32)], ct.c_int),
+        "ketgpu_tc_image": ([i32, vp, vp, u64, ct.POINTER(u64)], ct.c_int),
         "ketgpu_state_stream": ([vp], vp),
         "ketgpu_apply": ([vp, vp, u64, ct.POINTER(Options)], ct.c_int),
         "ketgpu_run": ([i32, vp, u64, ct.POINTER(Options), vp], ct.c_int),

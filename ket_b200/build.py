@@ -1,6 +1,7 @@
 """Build libket_b200.so in-tree (sm_100a only).
 
-``python -m ket_b200.build`` (or ``__graft_entry__.build()``) compiles every
+``python ket_b200/build.py`` (or ``__graft_entry__.build()``; not ``-m``, which imports
+the package and so the library being rebuilt) compiles every
 CUDA source under ket_b200/csrc with nvcc for ``compute_100a/sm_100a`` and the
 host sources with g++ (C++20), and links ``ket_b200/libket_b200.so`` with the
 CUDA runtime linked statically.  Objects go to ket_b200/_build; a source is

@@ -872,6 +872,20 @@ KB_API int ketgpu_plan_pass_tc_form(const ketgpu_plan* p, uint64_t index, int32_
   });
 }
 
+KB_API int ketgpu_tc_image(int32_t k, const double* mat, uint32_t* out, uint64_t capacity, uint64_t* words) {
+  return guard([&] {
+    need(mat != nullptr && words != nullptr && (out != nullptr || capacity == 0), "null argument");
+    if (!tc_supported(k)) fail(KETGPU_ERR_INVALID, "tensor-core blocks have k = 4, 5 or 6");
+    const size_t dim = size_t{1} << k;
+    std::vector<cplx> m(dim * dim);
+    for (size_t i = 0; i < dim * dim; ++i) m[i] = cplx(mat[2 * i], mat[2 * i + 1]);
+    std::vector<uint32_t> img;
+    build_tc_image(m, k, img);
+    *words = img.size();
+    std::memcpy(out, img.data(), std::min<uint64_t>(capacity, img.size()) * sizeof(uint32_t));
+  });
+}
+
 KB_API void* ketgpu_state_stream(const ketgpu_state* s) {
   return s ? reinterpret_cast<void*>(as_state(s)->stream) : nullptr;
 }

@@ -379,3 +379,50 @@ def test_six_qubit_blocks_copy_half_tiles():
         pp = Plan(28, c.to_ops(), ket.make_options("c64", "greedy", 6, True))
         tc = [i for i in range(pp.stats()["n_passes"]) if pp.pass_info(i)["tensor"]]
         assert pp.pass_tc_form(tc[0])["tma_dims"] == want, qs
+
+
+@pytest.mark.parametrize("k", [4, 5, 6])
+def test_tensor_core_b_image_split_and_layout(k):
+    """The B operand plans upload for a tensor-core block, built on the
+    host: B[kk][n] = real embedding of the block matrix (B[2c][2r] = Re M[r][c],
+    B[2c+1][2r] = -Im M, B[2c][2r+1] = Im M, B[2c+1][2r+1] = Re M), scaled by
+    2^sb with its largest entry in [2^14, 2^15); hi = fp16(x) and lo =
+    fp16(x - hi), both rounded to nearest even (numpy's float16 is the
+    reference), at the K-major 128-byte-swizzle offset of (row n, column kk)
+    in whole 128-byte atoms along K; sb last."""
+    from ket_b200 import _lib
+    dim = 1 << k
+    K = N = 2 * dim
+    rng = np.random.default_rng(k)
+    q, _ = np.linalg.qr(rng.standard_normal((dim, dim)) + 1j * rng.standard_normal((dim, dim)))
+    m = np.ascontiguousarray(q, dtype=np.complex128)
+    words = ct.c_uint64()
+    assert _lib.lib.ketgpu_tc_image(k, m.ctypes.data, None, 0, ct.byref(words)) == 0
+    out = np.zeros(words.value, dtype=np.uint32)
+    assert _lib.lib.ketgpu_tc_image(k, m.ctypes.data, out.ctypes.data, out.size, ct.byref(words)) == 0
+    img = (K + 63) // 64 * N * 128  # bytes per image
+    assert words.value * 4 == 2 * img + 16
+    raw = out.view(np.uint8)
+    hi = raw[:img].view(np.uint16)
+    lo = raw[img:2 * img].view(np.uint16)
+    sb = int(out[2 * img // 4].view(np.int32))
+    B = np.zeros((K, N))
+    B[0::2, 0::2] = m.real.T
+    B[1::2, 0::2] = -m.imag.T
+    B[0::2, 1::2] = m.imag.T
+    B[1::2, 1::2] = m.real.T
+    assert 2.0 ** 14 <= np.abs(B).max() * 2.0 ** sb < 2.0 ** 15
+    kk, n = np.meshgrid(np.arange(K), np.arange(N), indexing="ij")
+    off = (kk >> 6) * N * 128 + n * 128 + ((((kk & 63) >> 3) ^ (n & 7)) << 4) + (kk & 7) * 2
+    v = np.ldexp(B, sb)
+    h = v.astype(np.float16)
+    l_ = (v - h.astype(np.float64)).astype(np.float16)
+    assert np.array_equal(hi[off // 2], h.view(np.uint16))
+    assert np.array_equal(lo[off // 2], l_.view(np.uint16))
+    # every used 16-bit slot is addressed once; at k = 4 half of each atom row is unused
+    assert len(np.unique(off)) == K * N
+    # what the MMAs sum: hi + lo within 2^-22 of each scaled entry's magnitude
+    # (plus fp16's subnormal spacing for tiny entries)
+    err = np.abs(h.astype(np.float64) + l_.astype(np.float64) - v)
+    assert np.all(err <= np.abs(v) * 2.0 ** -22 + 2.0 ** -25)
+    assert _lib.lib.ketgpu_tc_image(3, m.ctypes.data, None, 0, ct.byref(words)) != 0
