@@ -581,7 +581,8 @@ double Pass::bytes(int n, size_t amp) const {
   const double dim = (double)(uint64_t{1} << n);
   if (kind == PassKind::Fused || kind == PassKind::Diagonal || kind == PassKind::SharedRun) return 2.0 * amp * dim;
   if (kind == PassKind::NormCapture) return amp * dim;
-  if (kind == PassKind::NormRestore) return 3.0 * amp * dim;
+  // the norm read (unless the block before summed it) plus the rescale
+  if (kind == PassKind::NormRestore) return (norm_out ? 2.0 : 3.0) * amp * dim;
   if (kind == PassKind::Phase) return 2.0 * amp * dim / (double)(uint64_t{1} << nfixed);
   // pair: two amplitudes per pair, both read and written
   return 2.0 * amp * 2.0 * dim / (double)(uint64_t{1} << nfixed);

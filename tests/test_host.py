@@ -426,3 +426,27 @@ def test_tensor_core_b_image_split_and_layout(k):
     err = np.abs(h.astype(np.float64) + l_.astype(np.float64) - v)
     assert np.all(err <= np.abs(v) * 2.0 ** -22 + 2.0 ** -25)
     assert _lib.lib.ketgpu_tc_image(3, m.ctypes.data, None, 0, ct.byref(words)) != 0
+
+
+def test_norm_passes_around_tensor_core_blocks():
+    """Plans with tensor-core blocks capture the norm first and restore it
+    last; when the last block is on the tensor cores it sums the norm as it
+    stores, so the restore moves 2 x the state (rescale) instead of 3 x
+    (norm read + rescale).  SIMT plans asked to renormalize keep the read."""
+    import ket_b200 as ket
+    from ket_b200.api import Plan
+    from ket_b200.workloads import random_brickwork
+    n = 20
+    ops = random_brickwork(n, 10).to_ops()
+    state = 8 * 2.0 ** n
+    p = Plan(n, ops, ket.make_options("c64", "greedy", 6, True))
+    kinds = [p.pass_info(i) for i in range(int(p.stats()["n_passes"]))]
+    assert kinds[0]["kind"] == 3 and kinds[-1]["kind"] == 3
+    assert kinds[-2]["kind"] == 2 and kinds[-2]["tensor"]
+    assert kinds[0]["bytes"] == state and kinds[-1]["bytes"] == 2 * state
+    q = Plan(n, ops, ket.make_options("c64", "greedy", 5, False, renormalize=1))
+    kq = [q.pass_info(i) for i in range(int(q.stats()["n_passes"]))]
+    assert kq[0]["kind"] == 3 and kq[-1]["kind"] == 3 and not kq[-2]["tensor"]
+    assert kq[-1]["bytes"] == 3 * state
+    r = Plan(n, ops, ket.make_options("c64", "greedy", 5, False))
+    assert all(r.pass_info(i)["kind"] != 3 for i in range(int(r.stats()["n_passes"])))
