@@ -167,6 +167,13 @@ int ketgpu_plan_pass_gates(const ketgpu_plan* p, uint64_t index, int32_t* gates,
  * no counterpart in ket. */
 int ketgpu_plan_pass_tc_form(const ketgpu_plan* p, uint64_t index, int32_t* tma_dims,
                              int32_t* direct);
+/* The FP64 matrix of dense-block pass `index` (2^k x 2^k complex, row-major,
+ * interleaved re, im; matrix bit b <-> the pass's qubit b), as the plan
+ * built it from the pass's gates.  Writes min(capacity, 2 * 4^k) doubles;
+ * *count receives 2 * 4^k.  KETGPU_ERR_INVALID for a pass that is not a
+ * dense block.  Host only; no counterpart in ket. */
+int ketgpu_plan_pass_matrix(const ketgpu_plan* p, uint64_t index, double* out, uint64_t capacity,
+                            uint64_t* count);
 /* The tensor-core B operand of a k-qubit block (k = 4, 5 or 6) as plans
  * upload it: the real embedding of `mat` (2^k x 2^k complex, row-major,
  * interleaved re, im) scaled by 2^sb (its largest entry into [2^14, 2^15)),

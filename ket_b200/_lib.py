@@ -83,6 +83,7 @@ def _load():
         "ketgpu_run_last_profile": ([vp], ct.c_int),
         "ketgpu_plan_pass_tc_form": ([vp, u64, ct.POINTER(i32), ct.POINTER(i32)], ct.c_int),
         "ketgpu_tc_image": ([i32, vp, vp, u64, ct.POINTER(u64)], ct.c_int),
+        "ketgpu_plan_pass_matrix": ([vp, u64, vp, u64, ct.POINTER(u64)], ct.c_int),
         "ketgpu_state_stream": ([vp], vp),
         "ketgpu_apply": ([vp, vp, u64, ct.POINTER(Options)], ct.c_int),
         "ketgpu_run": ([i32, vp, u64, ct.POINTER(Options), vp], ct.c_int),

@@ -89,8 +89,20 @@ void pauli_masks(int n, const char* pauli, uint64_t& flip, uint64_t& sign, int& 
   q = num_y % 4;
 }
 
+void upload_plan_copies(Plan& plan, int device);
+
+// Device copies of a plan's tables, once per plan and device.  They go up
+// with cudaMemcpy from pageable host vectors, which may return before the
+// data lands; the kernels that read them run on the states' non-blocking
+// streams, which do not wait for the legacy stream the copies use, so the
+// copies are waited for here.
 void upload_plan_matrices(Plan& plan, int device) {
   if (plan.device == device) return;
+  upload_plan_copies(plan, device);
+  KB_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+}
+
+void upload_plan_copies(Plan& plan, int device) {
   if (plan.device >= 0) fail(KETGPU_ERR_INVALID, "plan was prepared for another device");
   plan.device = device;
   for (const Pass& p : plan.passes)
@@ -869,6 +881,21 @@ KB_API int ketgpu_plan_pass_tc_form(const ketgpu_plan* p, uint64_t index, int32_
     tc_form(plan.n, ps, &t, &d);
     *tma_dims = t;
     *direct = d;
+  });
+}
+
+KB_API int ketgpu_plan_pass_matrix(const ketgpu_plan* p, uint64_t index, double* out, uint64_t capacity,
+                                   uint64_t* count) {
+  return guard([&] {
+    need(p != nullptr && count != nullptr && (out != nullptr || capacity == 0), "null argument");
+    const Plan& plan = *as_plan(p);
+    if (index >= plan.passes.size()) fail(KETGPU_ERR_OUT_OF_RANGE, "pass index out of range");
+    const Pass& ps = plan.passes[index];
+    if (ps.kind != PassKind::Fused) fail(KETGPU_ERR_INVALID, "pass is not a dense block");
+    const std::vector<cplx>& m = plan.matrices[ps.mat_index];
+    *count = 2 * m.size();
+    const uint64_t nd = std::min<uint64_t>(capacity, 2 * m.size());
+    for (uint64_t i = 0; i < nd; ++i) out[i] = (i & 1) ? m[i / 2].imag() : m[i / 2].real();
   });
 }
 

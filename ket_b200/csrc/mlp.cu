@@ -302,10 +302,12 @@ KB_API int ketgpu_mlp_create(uint64_t seed, ketgpu_mlp** out) {
     fill(OFF_W1, HID * IN, IN);
     fill(OFF_W2, HID * HID, HID);
     fill(OFF_W3, HID, HID);
-    KB_CUDA(cudaMemcpy(M->master, h.data(), NPARAM * sizeof(float), cudaMemcpyHostToDevice));
-    KB_CUDA(cudaMemset(M->m, 0, NPARAM * sizeof(float)));
-    KB_CUDA(cudaMemset(M->v, 0, NPARAM * sizeof(float)));
-    KB_CUDA(cudaMemset(M->grad, 0, NPARAM * sizeof(float)));
+    // on the model's own (non-blocking) stream, ahead of the kernels that
+    // read these buffers
+    KB_CUDA(cudaMemcpyAsync(M->master, h.data(), NPARAM * sizeof(float), cudaMemcpyHostToDevice, M->stream));
+    KB_CUDA(cudaMemsetAsync(M->m, 0, NPARAM * sizeof(float), M->stream));
+    KB_CUDA(cudaMemsetAsync(M->v, 0, NPARAM * sizeof(float), M->stream));
+    KB_CUDA(cudaMemsetAsync(M->grad, 0, NPARAM * sizeof(float), M->stream));
     mlp_sync_bf16<<<64, 256, 0, M->stream>>>(M->master, M->w, NPARAM);
     count_launch();
     KB_CUDA(cudaStreamSynchronize(M->stream));
@@ -338,6 +340,7 @@ KB_API int ketgpu_mlp_get_weights(const ketgpu_mlp* mp, float* w1, float* b1, fl
     if (!M) fail(KETGPU_ERR_INVALID, "model is null");
     DeviceGuard dg(M->device);
     std::vector<__nv_bfloat16> h(NPARAM);
+    KB_CUDA(cudaStreamSynchronize(M->stream));  // the model's kernels write M->w on its own stream
     KB_CUDA(cudaMemcpy(h.data(), M->w, NPARAM * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost));
     auto put = [&](float* dst, size_t off, size_t cnt) {
       if (dst)
@@ -365,7 +368,7 @@ KB_API int ketgpu_mlp_set_weights(ketgpu_mlp* mp, const float* w1, const float* 
     std::memcpy(&h[OFF_W3], w3, HID * sizeof(float));
     h[OFF_B3] = b3[0];
     DeviceGuard dg(M->device);
-    KB_CUDA(cudaMemcpy(M->master, h.data(), NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+    KB_CUDA(cudaMemcpyAsync(M->master, h.data(), NPARAM * sizeof(float), cudaMemcpyHostToDevice, M->stream));
     mlp_sync_bf16<<<64, 256, 0, M->stream>>>(M->master, M->w, NPARAM);
     count_launch();
     KB_CUDA(cudaStreamSynchronize(M->stream));

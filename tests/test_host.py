@@ -450,3 +450,34 @@ def test_norm_passes_around_tensor_core_blocks():
     assert kq[-1]["bytes"] == 3 * state
     r = Plan(n, ops, ket.make_options("c64", "greedy", 5, False))
     assert all(r.pass_info(i)["kind"] != 3 for i in range(int(r.stats()["n_passes"])))
+
+
+def test_plan_block_matrices_match_the_oracle(oracle, golden):
+    """Every dense block's FP64 matrix, as the planner built it (on host
+    threads, after partitioning), equals the oracle's product of the block's
+    gates; the plans are rebuilt many times, so a matrix written by the
+    wrong job or a race between the builders would show up."""
+    import ctypes as ct
+    import ket_b200 as ket
+    from ket_b200 import _lib
+    from ket_b200.api import Plan
+    from ket_b200.workloads import random_brickwork, random_mixed
+    g = golden("random_mixed")
+    cases = [(n, g[f"ops_{n}"]) for n in (6, 10, 12)]
+    cases += [(14, random_mixed(14, 12, seed=4).to_ops()), (20, random_brickwork(20, 12, seed=7).to_ops())]
+    for rep in range(20):
+        for n, ops in cases:
+            for prec, k, tc in (("c128", 5, True), ("c64", 6, True), ("c128", 3, True), ("c64", 4, False)):
+                p = Plan(n, ops, ket.make_options(prec, "greedy", k, tc))
+                for i in range(int(p.stats()["n_passes"])):
+                    if p.pass_info(i)["kind"] != 2:
+                        continue
+                    qs = p.pass_qubits(i)
+                    gates = p.pass_gates(i)
+                    cnt = ct.c_uint64()
+                    buf = np.zeros(2 << (2 * len(qs)))
+                    assert _lib.lib.ketgpu_plan_pass_matrix(p._h, i, buf.ctypes.data, buf.size, ct.byref(cnt)) == 0
+                    got = buf.view(np.complex128).reshape(1 << len(qs), 1 << len(qs))
+                    want = oracle.block_matrix(np.ascontiguousarray(ops[gates]), qs)
+                    assert np.abs(got - want).max() < 1e-12, (rep, n, prec, k, i)
+                p.close()
