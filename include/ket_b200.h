@@ -237,7 +237,8 @@ int ketgpu_expval_sum(const ketgpu_state* s, const double* coeffs,
  * are looked up, and so loaded onto the device, when the first state is
  * created there (ketgpu_state_create), which allocates anyway; the call
  * itself allocates nothing.  It synchronises the state's stream and copies
- * the per-term results to the host before returning.  At most
+ * the per-term results to the host before returning, so it blocks the host
+ * and cannot be used inside stream capture.  At most
  * KETGPU_NOALLOC_MAX_TERMS terms; more returns KETGPU_ERR_INVALID. */
 #define KETGPU_NOALLOC_MAX_TERMS 256
 int ketgpu_expval_sum_noalloc(const ketgpu_state* s, const double* coeffs,
