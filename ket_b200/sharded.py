@@ -21,9 +21,16 @@ The schedule is built on the host before anything runs; it depends only on
 the circuit and n, G, so every rank builds the same one and the ranks take
 the same collective steps in the same order.
 
-Scope: unitary gates (ket's H..CSWAP), run from |0...0>, the squared norm,
-and a gather of the whole state for checking.  ``schedule`` and
-``exchange_half`` are device-independent and tested with gloo ranks on CPU.
+Pauli expectations: a term's X and Y factors on global positions are first
+swapped to local positions (the state is unchanged, only the map moves); a Z
+factor on a global position is the sign of the rank's bit there; each rank
+then takes the local term's expectation over its own amplitudes and the
+ranks' values are summed.
+
+Scope: unitary gates (ket's H..CSWAP), run from |0...0>, Pauli terms and sums
+with at most L X/Y factors per term, the squared norm, and a gather of the
+whole state for checking.  ``schedule`` and ``exchange_half`` are
+device-independent and tested with gloo ranks on CPU.
 """
 from __future__ import annotations
 
@@ -167,6 +174,10 @@ class DeviceShard:
     def norm(self) -> float:
         return self.state.norm()
 
+    def expval(self, pauli: str) -> float:
+        """<psi|P|psi> over this rank's amplitudes (no normalisation)."""
+        return self.state.expval(pauli)
+
     def to_numpy(self) -> np.ndarray:
         return self.state.to_numpy()
 
@@ -216,16 +227,57 @@ class ShardedState:
         self.reset()
         return self.apply(circuit, options)
 
-    def norm(self) -> float:
-        """Squared norm of the whole state (sum over ranks)."""
+    def _sum_over_ranks(self, x: float) -> float:
         import torch
         import torch.distributed as dist
-        v = torch.tensor([self.shard.norm()], dtype=torch.float64)
+        v = torch.tensor([float(x)], dtype=torch.float64)
         if self.world > 1:
             if dist.get_backend(self.group) == "nccl":
                 v = v.cuda()
             dist.all_reduce(v, group=self.group)
         return float(v.item())
+
+    def norm(self) -> float:
+        """Squared norm of the whole state (sum over ranks)."""
+        return self._sum_over_ranks(self.shard.norm())
+
+    def expval(self, obs) -> float:
+        """<psi|P|psi> for a Pauli string (n characters of I X Y Z, the
+        rightmost for qubit 0, as ket writes them) or a sum of
+        (coefficient, string) terms."""
+        terms = [(1.0, obs)] if isinstance(obs, str) else [(float(c), str(p)) for c, p in obs]
+        return sum(c * self._expval_term(p) for c, p in terms)
+
+    def _expval_term(self, pauli: str) -> float:
+        n, L = self.n, self.local_qubits
+        if len(pauli) != n:
+            raise ValueError(f"Pauli string of length {len(pauli)} for {n} qubits")
+        ch = [pauli[n - 1 - q].upper() for q in range(n)]
+        if any(c not in "IXYZ" for c in ch):
+            raise ValueError("Pauli strings hold only I, X, Y and Z")
+        if sum(c in "XY" for c in ch) > L:
+            raise ValueError("a sharded state takes at most n - G X/Y factors per term")
+        at = [0] * n
+        for q, p in enumerate(self.pos):
+            at[p] = q
+        # X and Y factors must act on local positions: swap them in, giving
+        # way with local positions whose factor is I (else Z)
+        for q in range(n):
+            if ch[q] not in "XY" or self.pos[q] < L:
+                continue
+            victim = min((p for p in range(L) if ch[at[p]] not in "XY"), key=lambda p: (ch[at[p]] != "I", p))
+            g = self.pos[q]
+            self.shard.exchange(victim, g - L, self.rank, self.group)
+            self.swaps += 1
+            v = at[victim]
+            self.pos[q], self.pos[v] = victim, g
+            at[victim], at[g] = q, v
+        sign = 1.0
+        for q in range(n):
+            if ch[q] == "Z" and self.pos[q] >= L and (self.rank >> (self.pos[q] - L)) & 1:
+                sign = -sign
+        local = "".join(ch[at[p]] for p in range(L - 1, -1, -1))
+        return self._sum_over_ranks(sign * self.shard.expval(local))
 
     def gather(self) -> Optional[np.ndarray]:
         """The whole state in logical qubit order, on rank 0 (None elsewhere)."""

@@ -99,6 +99,9 @@ class OracleShard:
     def norm(self):
         return float(np.vdot(self.a, self.a).real)
 
+    def expval(self, pauli):
+        return self.oracle.expval(self.L, self.a, pauli)
+
     def to_numpy(self):
         return self.a.copy()
 
@@ -114,6 +117,11 @@ def _free_port():
     return p
 
 
+# n = 10: X/Y/Z on the top (global) qubits, on low ones, and mixed
+_PAULIS = ["XIIIIIIIIZ", "YZIIIIIIIX", "ZZIIIIIIII", "IIIIXYZIII", "XYZXYZIIII", "ZIIIIIIIIY", "IIIIIIIIII"]
+_COEFFS = [0.5, -1.25, 2.0, 0.75, -0.3, 1.1, 0.2]
+
+
 def _worker(rank, world, port, n, q):
     import datetime
     os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "MASTER_ADDR": "127.0.0.1",
@@ -126,7 +134,8 @@ def _worker(rank, world, port, n, q):
         G = world.bit_length() - 1
         s = ShardedState(n, shard=OracleShard(n - G))
         s.run(ops)
-        out.append((s.gather(), s.norm(), s.swaps))
+        ev = [s.expval(p) for p in _PAULIS] + [s.expval(list(zip(_COEFFS, _PAULIS)))]
+        out.append((s.gather(), s.norm(), s.swaps, ev))
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, out))
@@ -148,9 +157,13 @@ def test_sharded_run_on_gloo_ranks(oracle, world):
         assert p.exitcode == 0
     for i, ops in enumerate(_circuits(n)):
         want = oracle.run(n, ops, fuse=0)
-        got, norm, swaps = res[0][i]
+        got, norm, swaps, ev = res[0][i]
         assert np.abs(got - want).max() < 1e-12
         assert swaps > 0
+        exp = [oracle.expval(n, want, p) for p in _PAULIS]
+        exp.append(sum(c * e for c, e in zip(_COEFFS, exp)))
+        for r in range(world):
+            assert np.allclose(res[r][i][3], exp, atol=1e-12), (r, res[r][i][3], exp)
         for r in range(world):
             assert abs(res[r][i][1] - 1.0) < 1e-12  # every rank sees the all-reduced norm
             assert res[r][i][2] == swaps             # and took the same steps
