@@ -27,9 +27,17 @@ factor on a global position is the sign of the rank's bit there; each rank
 then takes the local term's expectation over its own amplitudes and the
 ranks' values are summed.
 
+Sampling is inverse-CDF sampling in physical index order, in two levels:
+a draw's uniform u (a position in the cumulative probability, as ket's
+measure takes it for a normalised state) picks the rank from the FP64
+running sum of the ranks' probabilities, and u less the mass of the ranks
+before it is drawn by the rank's own sampling tree; the physical index is
+mapped back to the logical qubits and the draws are gathered on rank 0 in
+their order.
+
 Scope: unitary gates (ket's H..CSWAP), run from |0...0>, Pauli terms and sums
-with at most L X/Y factors per term, the squared norm, and a gather of the
-whole state for checking.  ``schedule`` and ``exchange_half`` are
+with at most L X/Y factors per term, sampling, the squared norm, and a
+gather of the whole state for checking.  ``schedule`` and ``exchange_half`` are
 device-independent and tested with gloo ranks on CPU.
 """
 from __future__ import annotations
@@ -178,6 +186,12 @@ class DeviceShard:
         """<psi|P|psi> over this rank's amplitudes (no normalisation)."""
         return self.state.expval(pauli)
 
+    def sample(self, positions: np.ndarray) -> np.ndarray:
+        """Local indices drawn by the state's sampling tree for positions in
+        this rank's cumulative probability (absolute, like a uniform for a
+        normalised state)."""
+        return self.state.sample(positions)
+
     def to_numpy(self) -> np.ndarray:
         return self.state.to_numpy()
 
@@ -247,6 +261,49 @@ class ShardedState:
         (coefficient, string) terms."""
         terms = [(1.0, obs)] if isinstance(obs, str) else [(float(c), str(p)) for c, p in obs]
         return sum(c * self._expval_term(p) for c, p in terms)
+
+    def sample(self, uniforms) -> Optional[np.ndarray]:
+        """Basis-state indices (logical qubit order) drawn for the uniforms in
+        [0, 1), the same on every rank, as ket's measure draws them from a
+        normalised state; on rank 0 (None elsewhere)."""
+        import torch.distributed as dist
+        u = np.ascontiguousarray(uniforms, dtype=np.float64)
+        mine_p = float(self.shard.norm())
+        if self.world > 1:
+            tot = [None] * self.world
+            dist.all_gather_object(tot, mine_p, group=self.group)
+        else:
+            tot = [mine_p]
+        tot = np.array(tot, dtype=np.float64)
+        cum = np.cumsum(tot)
+        if not cum[-1] > 0:
+            raise ValueError("cannot sample a state of zero norm")
+        x = u
+        # the first rank whose running sum exceeds x (ranks without
+        # probability never qualify); x at the very top goes to the last
+        # rank with probability
+        last = int(np.nonzero(tot > 0)[0].max())
+        which = np.minimum(np.searchsorted(cum, x, side="right"), last)
+        sel = np.nonzero(which == self.rank)[0]
+        local = np.empty(0, dtype=np.uint64)
+        if len(sel):
+            lo = cum[self.rank] - tot[self.rank]
+            local = np.asarray(self.shard.sample(np.maximum(x[sel] - lo, 0.0)), dtype=np.uint64)
+        phys = (np.uint64(self.rank) << np.uint64(self.local_qubits)) | local
+        logical = np.zeros_like(phys)
+        for q, p in enumerate(self.pos):
+            logical |= ((phys >> np.uint64(p)) & np.uint64(1)) << np.uint64(q)
+        if self.world > 1:
+            parts = [None] * self.world if self.rank == 0 else None
+            dist.gather_object((sel, logical), parts, dst=0, group=self.group)
+        else:
+            parts = [(sel, logical)]
+        if self.rank != 0:
+            return None
+        out = np.empty(len(u), dtype=np.uint64)
+        for sl, lg in parts:
+            out[sl] = lg
+        return out
 
     def _expval_term(self, pauli: str) -> float:
         n, L = self.n, self.local_qubits

@@ -102,6 +102,9 @@ class OracleShard:
     def expval(self, pauli):
         return self.oracle.expval(self.L, self.a, pauli)
 
+    def sample(self, u):
+        return self.oracle.sample_tree(self.L, self.a, u)
+
     def to_numpy(self):
         return self.a.copy()
 
@@ -135,7 +138,8 @@ def _worker(rank, world, port, n, q):
         s = ShardedState(n, shard=OracleShard(n - G))
         s.run(ops)
         ev = [s.expval(p) for p in _PAULIS] + [s.expval(list(zip(_COEFFS, _PAULIS)))]
-        out.append((s.gather(), s.norm(), s.swaps, ev))
+        draws = s.sample(np.random.default_rng(17).random(20000))
+        out.append((s.gather(), s.norm(), s.swaps, ev, draws, list(s.pos)))
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, out))
@@ -157,13 +161,35 @@ def test_sharded_run_on_gloo_ranks(oracle, world):
         assert p.exitcode == 0
     for i, ops in enumerate(_circuits(n)):
         want = oracle.run(n, ops, fuse=0)
-        got, norm, swaps, ev = res[0][i]
+        got, norm, swaps, ev, _, pos = res[0][i]
         assert np.abs(got - want).max() < 1e-12
         assert swaps > 0
         exp = [oracle.expval(n, want, p) for p in _PAULIS]
         exp.append(sum(c * e for c, e in zip(_COEFFS, exp)))
         for r in range(world):
             assert np.allclose(res[r][i][3], exp, atol=1e-12), (r, res[r][i][3], exp)
+            if r:
+                assert res[r][i][4] is None
+        # draws: valid outcomes, distributed as |psi|^2 -- counts within 6
+        # sigma plus 3 (outcomes with a fraction of an expected draw are in
+        # the Poisson regime, where one draw is not an outlier)
+        draws = res[0][i][4]
+        p = np.abs(want) ** 2
+        N = len(draws)
+        assert N == 20000 and np.all(p[draws.astype(np.int64)] > 0)
+        counts = np.bincount(draws.astype(np.int64), minlength=1 << n)
+        assert np.all(np.abs(counts - N * p) <= 6 * np.sqrt(N * p * (1 - p)) + 3)
+        # and they are the inverse CDF of the state in physical index order
+        # (the ranks' trees sum in another order than numpy, so a draw on a
+        # boundary may differ by rounding)
+        idx = np.arange(1 << n)
+        lidx = np.zeros_like(idx)
+        for qq, pp in enumerate(pos):
+            lidx |= ((idx >> pp) & 1) << qq
+        cdf = np.cumsum(np.abs(got[lidx]) ** 2)
+        u = np.random.default_rng(17).random(N)
+        ref = lidx[np.minimum(np.searchsorted(cdf, u, side="right"), (1 << n) - 1)]
+        assert np.sum(ref != draws.astype(np.int64)) <= 5
         for r in range(world):
             assert abs(res[r][i][1] - 1.0) < 1e-12  # every rank sees the all-reduced norm
             assert res[r][i][2] == swaps             # and took the same steps
