@@ -256,3 +256,23 @@ def test_sharded_state_on_one_rank_is_the_device_state(oracle):
     want = oracle.run(n, ops, fuse=0)
     assert np.abs(got - want).max() < 1e-5
     s.close()
+
+
+def test_schedule_with_three_local_qubits(oracle):
+    """The fewest local qubits a sharded state allows (3): a 3-qubit gate on
+    global qubits swaps every local position out."""
+    from ket_b200 import sharded
+    from ket_b200.circuit import Circuit
+    from ket_b200.workloads import random_mixed
+    n, G = 6, 3
+    c = Circuit(n)
+    c.h(3)
+    c.h(4)
+    c.h(5)
+    c.ccx(3, 4, 5)
+    c.cswap(5, 0, 4)
+    ops = np.concatenate([c.to_ops(), random_mixed(n, 6, seed=9).to_ops()])
+    steps, pos = sharded.schedule(n, G, ops)
+    got, swaps = _emulate(n, G, ops, oracle)
+    assert np.abs(got - oracle.run(n, ops, fuse=0)).max() < 1e-12
+    assert swaps >= 3
