@@ -91,7 +91,7 @@ TARGETS = {
     "low5": [0, 1, 2, 3, 4], "high5": None, "mixed5": [0, 3, 7, 11, 13], "spread5": [1, 5, 8, 12, 15],
     "q1tgt5": [1, 6, 9, 12, 14], "q2tgt5": [2, 7, 9, 11, 13],
     "low4": [0, 1, 2, 3], "mixed4": [2, 6, 9, 14], "high4": None, "q3tgt4": [3, 7, 10, 14],
-    # k = 6: two MMA passes of half the output columns per tile, one A region
+    # k = 6: half-tile tensor copies (cp.async when qubit 0 is a target), two A regions, N = 128
     "low6": [0, 1, 2, 3, 4, 5], "high6": None, "mixed6": [0, 3, 7, 11, 13, 15],
     "spread6": [1, 5, 8, 12, 15, 17], "q1tgt6": [1, 6, 9, 12, 14, 15], "q2tgt6": [2, 7, 9, 11, 13, 15],
     "q2run6": [2, 3, 4, 5, 6, 7], "q6run6": [6, 7, 8, 9, 10, 11],
