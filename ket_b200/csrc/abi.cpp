@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <mutex>
 #include <random>
@@ -135,7 +136,9 @@ void upload_plan_copies(Plan& plan, int device) {
   if (plan.matrices.empty()) return;
   std::vector<double> h64;
   std::vector<float> h32;
-  std::vector<uint32_t> htc, img;
+  std::vector<uint32_t> htc;
+  std::vector<size_t> tc_jobs;
+  size_t tc_words = 0;
   plan.off64.assign(plan.matrices.size(), 0);
   plan.off32.assign(plan.matrices.size(), 0);
   plan.offtc.assign(plan.matrices.size(), 0);
@@ -159,10 +162,10 @@ void upload_plan_copies(Plan& plan, int device) {
         }
       while (h64.size() % 2) h64.push_back(0);
     } else if (tensor[i]) {
-      plan.offtc[i] = htc.size() * sizeof(uint32_t);
-      build_tc_image(m, kof[i], img);
-      htc.insert(htc.end(), img.begin(), img.end());
-      while (htc.size() % 64) htc.push_back(0);  // 256-byte alignment
+      // place now, build below on host threads
+      plan.offtc[i] = tc_words * sizeof(uint32_t);
+      tc_jobs.push_back(i);
+      tc_words += (tc_image_bytes(kof[i]) / 4 + 63) / 64 * 64;  // 256-byte alignment
     } else {
       plan.off32[i] = h32.size() * sizeof(float);
       for (int c = 0; c < dim; ++c)
@@ -180,6 +183,38 @@ void upload_plan_copies(Plan& plan, int device) {
   if (!h32.empty()) {
     KB_CUDA(cudaMalloc(&plan.d_mat32, h32.size() * sizeof(float)));
     KB_CUDA(cudaMemcpy(plan.d_mat32, h32.data(), h32.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (!tc_jobs.empty()) {
+    // tensor-core B images (fp16 splits of every entry) on host threads,
+    // each written at its place in htc
+    htc.assign(tc_words, 0u);
+    auto build = [&](size_t i) {
+      std::vector<uint32_t> img;
+      build_tc_image(plan.matrices[i], kof[i], img);
+      std::memcpy(htc.data() + plan.offtc[i] / sizeof(uint32_t), img.data(), img.size() * sizeof(uint32_t));
+    };
+    const unsigned nt = tc_jobs.size() < 4 ? 1u
+                        : std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+    if (nt <= 1) {
+      for (size_t i : tc_jobs) build(i);
+    } else {
+      std::atomic<size_t> next{0};
+      std::exception_ptr err;
+      std::atomic<bool> failed{false};
+      std::vector<std::thread> th;
+      for (unsigned t = 0; t < nt; ++t)
+        th.emplace_back([&] {
+          for (size_t j; (j = next.fetch_add(1)) < tc_jobs.size();) {
+            try {
+              build(tc_jobs[j]);
+            } catch (...) {
+              if (!failed.exchange(true)) err = std::current_exception();
+            }
+          }
+        });
+      for (auto& x : th) x.join();
+      if (err) std::rethrow_exception(err);
+    }
   }
   if (!htc.empty()) {
     KB_CUDA(cudaMalloc(&plan.d_tc, htc.size() * sizeof(uint32_t)));

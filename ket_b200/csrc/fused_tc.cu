@@ -1092,29 +1092,43 @@ void launch_tc(const State& st, const Pass& p, const void* b_image, double* norm
   KB_CUDA(cudaGetLastError());
 }
 
-// IEEE binary16 bits of v, rounded to nearest, ties to even (host only).
+// IEEE binary16 bits of v, rounded to nearest, ties to even (host only), by
+// integer operations on the double's fields: keep the top 11 significant
+// bits (fewer below 2^-14, where the spacing is 2^-24), round on the bits
+// dropped, and let a carry move the exponent.
 uint16_t host_f16_bits(double v) {
-  const uint16_t sign = std::signbit(v) ? 0x8000u : 0u;
-  const double a = std::fabs(v);
-  if (a == 0) return sign;
-  if (!(a < 65520.0)) return (uint16_t)(sign | 0x7c00u);  // rounds to infinity
-  int ex;
-  std::frexp(a, &ex);  // a in [2^(ex-1), 2^ex)
-  int e = ex - 1;
-  if (e < -14) e = -14;  // subnormals: spacing 2^-24
-  double m = std::nearbyint(std::ldexp(a, 10 - e));  // significand in units of 2^(e-10)
-  if (m >= 2048) {
-    m /= 2;
-    ++e;
+  uint64_t b;
+  std::memcpy(&b, &v, 8);
+  const uint16_t sign = (uint16_t)((b >> 48) & 0x8000u);
+  b &= 0x7fffffffffffffffull;
+  if (b > 0x7ff0000000000000ull) return (uint16_t)(sign | 0x7e00u);  // NaN
+  const int e = (int)(b >> 52) - 1023;  // v in [2^e, 2^(e+1)) for normal doubles
+  if (e > 15) return (uint16_t)(sign | 0x7c00u);  // 2^16 and up, infinity
+  if (e < -25) return sign;                        // below half the least subnormal
+  const uint64_t m = (b & ((uint64_t{1} << 52) - 1)) | (uint64_t{1} << 52);  // 53-bit significand
+  const int shift = e >= -14 ? 42 : 42 + (-14 - e);  // bits dropped
+  uint64_t q = m >> shift;
+  const uint64_t rem = m & ((uint64_t{1} << shift) - 1), half = uint64_t{1} << (shift - 1);
+  if (rem > half || (rem == half && (q & 1))) ++q;
+  if (e < -14) return (uint16_t)(sign | q);  // subnormal (q = 1024: the least normal)
+  int E = e;
+  if (q == 2048) {
+    q = 1024;
+    ++E;
   }
-  if (e > 15) return (uint16_t)(sign | 0x7c00u);
-  if (m < 1024) return (uint16_t)(sign | (uint16_t)m);  // subnormal (e = -14)
-  return (uint16_t)(sign | ((e + 15) << 10) | ((int)m - 1024));
+  if (E > 15) return (uint16_t)(sign | 0x7c00u);
+  return (uint16_t)(sign | ((E + 15) << 10) | (q - 1024));
 }
 
 double host_f16_value(uint16_t h) {
   const int ex = (h >> 10) & 31, man = h & 1023;
-  const double v = ex == 0 ? std::ldexp((double)man, -24) : std::ldexp((double)(1024 + man), ex - 25);
+  double v;
+  if (ex == 0) {
+    v = man * 5.9604644775390625e-08;  // man * 2^-24, exact
+  } else {
+    const uint64_t bits = ((uint64_t)(ex - 15 + 1023) << 52) | ((uint64_t)man << 42);
+    std::memcpy(&v, &bits, 8);
+  }
   return (h & 0x8000u) ? -v : v;
 }
 
@@ -1145,6 +1159,7 @@ void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& 
   const size_t img = (tc_image_bytes(k) - 16) / 2;
   unsigned char* hi = reinterpret_cast<unsigned char*>(out.data());
   unsigned char* lo = hi + img;
+  const double scale = std::ldexp(1.0, sb);  // a power of two: exact products
   for (int n = 0; n < N; ++n)
     for (int kk = 0; kk < K; ++kk) {
       const int r = n >> 1, c = kk >> 1;
@@ -1152,7 +1167,7 @@ void build_tc_image(const std::vector<cplx>& mat, int k, std::vector<uint32_t>& 
       double v;
       if ((n & 1) == 0) v = (kk & 1) == 0 ? m.real() : -m.imag();
       else v = (kk & 1) == 0 ? m.imag() : m.real();
-      v = std::ldexp(v, sb);
+      v *= scale;
       const uint16_t h = host_f16_bits(v);
       const uint16_t l = host_f16_bits(v - host_f16_value(h));
       const uint32_t off = sw128_offset_h(n, kk, N);
