@@ -276,3 +276,28 @@ def test_schedule_with_three_local_qubits(oracle):
     got, swaps = _emulate(n, G, ops, oracle)
     assert np.abs(got - oracle.run(n, ops, fuse=0)).max() < 1e-12
     assert swaps >= 3
+
+
+def test_schedule_property_over_random_circuits(oracle):
+    """Property check of the swap schedule: for random circuits, register
+    sizes and numbers of global qubits, running the steps on the ranks'
+    slices reproduces the unsharded state, and running the same circuit again
+    from the map the first run left (a second apply) still does."""
+    from ket_b200 import sharded
+    from ket_b200.workloads import random_mixed
+    rng = np.random.default_rng(2024)
+    for trial in range(24):
+        n = int(rng.integers(6, 12))
+        G = int(rng.integers(1, min(4, n - 3) + 1))
+        ops = random_mixed(n, int(rng.integers(2, 10)), seed=int(rng.integers(1 << 30))).to_ops()
+        got, _ = _emulate(n, G, ops, oracle)
+        assert np.abs(got - oracle.run(n, ops, fuse=0)).max() < 1e-12, (trial, n, G)
+        # a second application starting from the first run's map
+        steps1, pos1 = sharded.schedule(n, G, ops)
+        steps2, pos2 = sharded.schedule(n, G, ops, start=pos1)
+        assert sorted(pos2) == list(range(n))
+        for st in steps2:
+            if isinstance(st, sharded.Apply):
+                for o in st.ops:
+                    a = 1 if o["type"] <= 11 else (2 if o["type"] <= 21 else 3)
+                    assert all(int(o["q"][j]) < n - G for j in range(a))
